@@ -1,0 +1,169 @@
+/*
+ * pcom_gpu.h -- C ABI of the B200 (sm_100a) implementation of the PCOM v2.2
+ * baroclinic time step (ouyuyuan/pcom).
+ *
+ * The reference has no plugin/FFI layer: its hot path is the per-step call
+ * block of main.f90:205-223 (den_alpha, int_pgra, int_readyc, int_trop,
+ * int_clin, int_ssh, int_ts) plus the daily den_prho (main.f90:179,200),
+ * operating on module-global arrays (mod_arrays.f90:28-122).  This header is
+ * the drop-in boundary for that block: a Fortran driver binds it with
+ * ISO_C_BINDING and keeps its own setup, calendar, namelist
+ * and netCDF I/O.
+ *
+ * Conventions
+ *  - Every array is a plain host pointer in Fortran order (i fastest) over the
+ *    padded local domain ni x nj [x nk | x nkp], ni = glo_ni + 2, nj = glo_nj + 2
+ *    (mod_param.f90:332-342 with npx = npy = 1).  type_mat arrays are AoS
+ *    pairs (x(1), x(2)) per point (mod_type.f90:75-77).
+ *  - Every function returns 0 on success or a PCOM_ERR_* code; the message of
+ *    the last error is available from pcom_gpu_last_error().  Nothing here
+ *    calls exit(): the Fortran side turns a nonzero status into `stop`, as the
+ *    reference does for its own errors (mod_io.f90:546-549).
+ *  - One handle = one model domain = one CUDA stream.  Calls are synchronous
+ *    at return unless the name says _async.
+ */
+#ifndef PCOM_GPU_H
+#define PCOM_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCOM_OK 0
+#define PCOM_ERR_ARG 1      /* bad argument, size or inconsistent static data */
+#define PCOM_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define PCOM_ERR_STATE 3    /* call out of order (e.g. step before upload_static) */
+#define PCOM_ERR_NUMERIC 4  /* the NaN/Inf watchdog tripped */
+#define PCOM_ERR_TIMEOUT 5  /* a bounded device-side wait gave up */
+
+/* pcom_dims.flags */
+#define PCOM_PREC_FP64 0x0   /* FP64 everywhere: the reference's arithmetic */
+#define PCOM_PREC_MIXED 0x1  /* FP32 stencils, FP64 bottom-pressure accumulation */
+#define PCOM_LIT_R8 0x10     /* default-REAL literals read as REAL(8) (ifort -r8);
+                                otherwise REAL(4) as gfortran compiles them */
+
+typedef struct pcom_handle pcom_handle;
+
+/* Sizes and time steps.  Replaces the dimension/namelist globals of
+ * mod_param.f90:40-81 (glo_ni, glo_nj, nk, ni, nj, nm%bt, nm%bc, nm%rst). */
+typedef struct pcom_dims {
+  int32_t glo_ni, glo_nj, nk;
+  int32_t ni, nj;          /* must equal glo_ni + 2, glo_nj + 2 */
+  int32_t dtbt, dtbc;      /* barotropic / baroclinic step (s) */
+  int32_t flags;           /* PCOM_PREC_* | PCOM_LIT_R8 */
+  int32_t rst;             /* nm%rst: 1 = restart run (skips the AB3 start-up) */
+  int32_t reserved[3];
+} pcom_dims;
+
+/* Static grid data, uploaded once (main.f90:105-122 computes it).
+ * rh[g], tn[g]: ni*nj, dx[g]: AoS ni*nj*2 for g = grid 1..4 (type_gi,
+ * mod_type.f90:97-108), in the order g1j, g2j, g3j, g4j.
+ * z1/pr1/dz1/dpr1: nkp (gi1); z2/pr2/dz2/dpr2: nk (gi2) (type_gj).
+ * msk_t, msk_u: ni*nj*nk int32; lev_t, lev_u: ni*nj int32; phih and prh:
+ * ni*nj; suffix _t = T grid (g12), _u = U grid (g32) (type_gij).  cv1, cv2, cor, graphihx,
+ * graphihy: ni*nj (U grid).  km, kh: ni*nj*nkp. */
+typedef struct pcom_static {
+  const double *rh[4], *tn[4], *dx[4];
+  const double *z1, *pr1, *dz1, *dpr1;
+  const double *z2, *pr2, *dz2, *dpr2;
+  const int32_t *msk_t, *lev_t, *msk_u, *lev_u;
+  const double *phih_t, *prh_t, *phih_u, *prh_u;
+  const double *cv1, *cv2, *cor;
+  const double *km, *kh;
+  const double *graphihx, *graphihy;
+} pcom_static;
+
+/* Prognostic and carried state (mod_arrays.f90:80-116).  Any pointer may be
+ * NULL to skip that field.  3D fields are ni*nj*nk except wm (ni*nj*nkp) and
+ * prho (AoS ni*nj*nk*2).  chc..mch2 are the four levels of `ch`
+ * (mod_arrays.f90:433-436). */
+typedef struct pcom_state {
+  double *tc, *sc, *tp, *sp;
+  double *uc, *vc, *up, *vp;
+  double *auc, *aup, *aupp, *avc, *avp, *avpp;
+  double *ubc, *vbc, *ubp, *vbp;
+  double *chc, *chp, *mch, *mch2;
+  double *am;
+  double *prho;
+  double *alpha, *adp;
+  double *wm;
+} pcom_state;
+
+/* Daily surface forcing after int_bnd (mod_int.f90:649-691), ni*nj each. */
+typedef struct pcom_forcing {
+  const double *taux, *tauy, *t, *s, *pa, *fw;
+} pcom_forcing;
+
+/* Time-mean accumulators and their record counters (eqts%act/acs/acr,
+ * equv%acu/acv, eqw%acw, eqch%acch, acssh; mod_type.f90:155-205). */
+typedef struct pcom_accum {
+  double *act, *acs, *acr, *acu, *acv, *acw;
+  double *acch, *acssh;
+  int32_t n_ts, n_uv, n_w, n_ch, n_ssh;
+} pcom_accum;
+
+/* --- lifetime ------------------------------------------------------------ */
+/* Replaces arrays_allocate (mod_arrays.f90:142-352) for the device mirrors. */
+int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out);
+int pcom_gpu_destroy(pcom_handle *h);
+
+/* --- data movement ------------------------------------------------------- */
+/* Grid data computed by set_hgrid/set_vgrid/set_grid/calc_cf/inistat
+ * (main.f90:408-704).  Masks must be the ones set_grid builds
+ * (msk = lev >= k); any other mask is rejected with PCOM_ERR_ARG. */
+int pcom_gpu_upload_static(pcom_handle *h, const pcom_static *s);
+/* State in/out: at start-up (inistat, main.f90:675-704), restart read
+ * (input_rst, mod_mympi.f90:460-478) and restart write (merge_out_rst,
+ * mod_mympi.f90:133-176). */
+int pcom_gpu_set_state(pcom_handle *h, const pcom_state *s);
+int pcom_gpu_get_state(pcom_handle *h, pcom_state *s);
+/* bnd%* after int_bnd or the 6-hourly file reads (main.f90:164-201). */
+int pcom_gpu_set_forcing(pcom_handle *h, const pcom_forcing *f);
+/* Accumulators for output() (main.f90:726-760) and their reset. */
+int pcom_gpu_get_accum(pcom_handle *h, pcom_accum *a);
+int pcom_gpu_reset_accum(pcom_handle *h);
+
+/* --- compute ------------------------------------------------------------- */
+/* den_prho (mod_den.f90:120-153): daily density derivatives. */
+int pcom_gpu_den_prho(pcom_handle *h);
+/* One baroclinic step: main.f90:205-223 in order.  tctr_i is tctr%i, the
+ * 1-based step counter that drives the AB3 start-up (mod_int.f90:122-132). */
+int pcom_gpu_step(pcom_handle *h, int64_t tctr_i);
+/* The same, enqueued on the handle's stream without waiting. */
+int pcom_gpu_step_async(pcom_handle *h, int64_t tctr_i);
+/* One subroutine of the step, for bisection against a CPU run:
+ * 0 den_alpha (main.f90:205), 1 int_pgra, 2 int_readyc, 3 int_trop,
+ * 4 int_clin, 5 int_ssh, 6 int_ts (mod_int.f90:64-507). */
+int pcom_gpu_phase(pcom_handle *h, int32_t phase, int64_t tctr_i);
+
+/* --- diagnostics --------------------------------------------------------- */
+/* Copy a named device array (state, intermediate or static) to host.
+ * n is the capacity of `host` in doubles; returns PCOM_ERR_ARG if too small
+ * or unknown.  Names: the pcom_state/pcom_accum members plus fx, fy, pax,
+ * pay, ut, vt, bphi_xn/xs/ye/yw, bgraphi_xn/xs/ye/yw. */
+int pcom_gpu_get_field(pcom_handle *h, const char *name, double *host, int64_t n);
+/* Element count of a named array (0 if unknown). */
+int64_t pcom_gpu_field_size(pcom_handle *h, const char *name);
+/* Run the NaN/Inf watchdog over the prognostic fields; PCOM_ERR_NUMERIC if
+ * any wet point is not finite. */
+int pcom_gpu_check_finite(pcom_handle *h);
+
+/* --- streams and timing -------------------------------------------------- */
+/* Use an external CUDA stream (cudaStream_t as void*) for all work. */
+int pcom_gpu_set_stream(pcom_handle *h, void *stream);
+int pcom_gpu_sync(pcom_handle *h);
+/* Per-kernel device timing with CUDA events (off by default).  When on,
+ * pcom_gpu_profile_read fills up to `cap` entries of names (64 chars each),
+ * launch counts and total milliseconds and returns the entry count. */
+int pcom_gpu_profile(pcom_handle *h, int32_t enable);
+int pcom_gpu_profile_read(pcom_handle *h, char *names, int64_t *launches, double *ms, int32_t cap);
+/* Number of this library's kernel launches issued so far on this handle. */
+int64_t pcom_gpu_launch_count(pcom_handle *h);
+
+/* Message of the last failed call on this thread. */
+int pcom_gpu_last_error(char *buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

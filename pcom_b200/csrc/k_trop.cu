@@ -1,0 +1,382 @@
+// k_trop.cu -- the barotropic predictor/corrector subcycle of int_trop
+// (mod_int.f90:153-296) as ONE persistent cooperative kernel.
+//
+// The 2-D domain (interior columns x all rows) is cut into TX x TY tiles.
+// Each CTA owns tiles; for every substep it stages a (TX+4) x (TY+4) region of
+// the previous substep's (ch, ub, vb) in shared memory, evaluates the
+// predictor ch, the viscosity, the bottom-pressure gradient forces, the
+// Coriolis-adjusted corrector velocity and the corrector ch for its tile
+// (recomputing the 1-2 cell halo of intermediates instead of exchanging
+// them), writes (ch, ub, vb) for the tile to a ping-pong buffer in L2, and
+// meets the other CTAs at one grid barrier per substep.  The 120 substeps of
+// a 3600 s / 60 s step therefore cost 120 grid barriers and no launches.
+//
+// The grid barrier is a counter/generation pair with a bounded spin: if a
+// wait exceeds its iteration limit the kernel records PCOM_ERR_TIMEOUT in
+// err[0] and every CTA returns at its next barrier.  The launch is
+// cooperative, so all CTAs are co-resident and the limit is never reached in
+// normal operation.
+#include <cuda/atomic>
+#include "pcom_dev.cuh"
+#include "pcom_kernels.h"
+
+namespace {
+
+constexpr long long kSpinLimit = 1LL << 26;  // ~seconds with the nanosleep below
+
+__device__ bool grid_barrier(const Dev &P, unsigned nblocks) {
+  __syncthreads();
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(P.bar[0]);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(P.bar[1]);
+    cuda::atomic_ref<int, cuda::thread_scope_device> err(P.err[0]);
+    int fail = err.load(cuda::memory_order_relaxed) != 0;
+    if (!fail) {
+      const unsigned g = gen.load(cuda::memory_order_acquire);
+      const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+      if (arrived == nblocks - 1) {
+        cnt.store(0u, cuda::memory_order_relaxed);
+        gen.fetch_add(1u, cuda::memory_order_release);
+      } else {
+        long long it = 0;
+        while (gen.load(cuda::memory_order_acquire) == g) {
+          if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
+            err.store(1, cuda::memory_order_relaxed);
+            fail = 1;
+            break;
+          }
+          if (it > 64) __nanosleep(64);
+        }
+      }
+    }
+    s_fail = fail;
+  }
+  __syncthreads();
+  return s_fail == 0;
+}
+
+// field slots in shared memory
+enum {
+  F_CH, F_UB, F_VB,          // previous substep state (T, U, U)
+  F_S1, F_X2,                // supb1, supb2*rh3 (U)
+  F_TE, F_TN,                // ter to E / N of the above
+  F_PRED,                    // predictor ch (T)
+  F_SCHE,                    // sqrt(ter(pred)) (U)
+  F_A1U, F_A1V, F_GY, F_CN,  // N-grid intermediates
+  F_A2U, F_A2V, F_GX, F_CE,  // E-grid intermediates
+  F_UBC, F_VBC, F_S1N, F_X2N, F_TEN, F_TNN,
+  F_COUNT
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(256, 1) k_trop(const __grid_constant__ Dev P, int TX, int TY, int ntx, int nty) {
+  extern __shared__ double smem[];
+  const int ni = P.ni, nj = P.nj, njm = P.njm, G = P.glo_ni;
+  const int W = TX + 4, H = TY + 4, RS = W * H;
+  const double a = P.c.a, bt = (double)P.bt, gamma_b = P.c.gamma_b;
+  const int nstep = P.nstep;
+  const int ntiles = ntx * nty;
+  const unsigned nblocks = gridDim.x;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // accumulators and the first substep's viscosity live in 2-D scratch (one per point)
+  double *A_mch = P.tr_acc[0], *A_mch2 = P.tr_acc[1], *A_ua = P.tr_acc[2], *A_va = P.tr_acc[3];
+  double *VS0U = P.tr_acc[4], *VS0V = P.tr_acc[5];
+
+  auto S = [&](int f, int lx, int ly) -> double & { return smem[f * RS + ly * W + lx]; };
+  auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
+
+  // initialise accumulators for owned points: mch = mch2 = chc, ua = ubc, va = vbc
+  for (int t = blockIdx.x; t < ntiles; t += nblocks) {
+    const int tx = t % ntx, ty = t / ntx;
+    const int R0 = tx * TX, J0 = ty * TY + 1;
+    const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+    for (int p = tid; p < tw * th; p += nth) {
+      const int i = R0 + (p % tw) + 2, j = J0 + p / tw;
+      const long long q = I2(P, i, j);
+      A_mch[q] = P.chc[q];
+      A_mch2[q] = P.chc[q];
+      A_ua[q] = P.ubc[q];
+      A_va[q] = P.vbc[q];
+    }
+  }
+  // (no barrier needed: accumulators are point-private)
+
+  for (int nt = 1; nt <= nstep; ++nt) {
+    const int d = (nt - 1) & 1;
+    const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
+    const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
+    const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
+    double *dst_ch = P.tr_ch[d], *dst_ub = P.tr_ub[d], *dst_vb = P.tr_vb[d];
+    const double *land_ch = (nt == 1) ? P.chc : src_ch;  // chc before the predictor
+
+    for (int t = blockIdx.x; t < ntiles; t += nblocks) {
+      const int tx = t % ntx, ty = t / ntx;
+      const int R0 = tx * TX, J0 = ty * TY + 1;
+      const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+      const int rr0 = R0 - 2, jj0 = J0 - 2;  // region origin
+      // --- S1: load ch (T, region [0, tw+4) x [0, th+4)) and ub, vb (U, [0, tw+3) x [0, th+3))
+      {
+        const int nx = tw + 4, ny = th + 4;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = p % nx, ly = p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          const long long q = I2(P, ring_i(rr0 + lx), j);
+          S(F_CH, lx, ly) = src_ch[q];
+          if (lx < tw + 3 && ly < th + 3) {
+            S(F_UB, lx, ly) = src_ub[q];
+            S(F_VB, lx, ly) = src_vb[q];
+          }
+        }
+      }
+      __syncthreads();
+      // --- S2: sch, supb on U [0, tw+3) x [0, th+3)
+      {
+        const int nx = tw + 3, ny = th + 3;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = p % nx, ly = p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          const long long q = I2(P, ring_i(rr0 + lx), j);
+          double sch = 1.0;
+          if (__ldg(P.lev_u + q) > 0) {
+            const double w = (j <= njm)
+                                 ? (S(F_CH, lx, ly) + S(F_CH, lx, ly + 1) + S(F_CH, lx + 1, ly) + S(F_CH, lx + 1, ly + 1)) * 0.25
+                                 : 0.0;
+            sch = sqrt(w);
+          }
+          const double ps = ld(P.prh_u, q) * sch;
+          S(F_S1, lx, ly) = ps * S(F_UB, lx, ly);
+          S(F_X2, lx, ly) = ps * S(F_VB, lx, ly) * ld(P.rh[3], q);
+        }
+      }
+      __syncthreads();
+      // --- S3: tE on E [0, tw+3) x [1, th+3); tN on N [1, tw+3) x [0, th+3)
+      {
+        const int nx = tw + 3, ny = th + 3;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = p % nx, ly = p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          if (ly >= 1) S(F_TE, lx, ly) = (j >= 2) ? 0.5 * (S(F_S1, lx, ly - 1) + S(F_S1, lx, ly)) : 0.0;
+          if (lx >= 1) S(F_TN, lx, ly) = 0.5 * (S(F_X2, lx - 1, ly) + S(F_X2, lx, ly));
+        }
+      }
+      __syncthreads();
+      // --- S4: predictor ch on T [1, tw+3) x [1, th+3)
+      {
+        const int nx = tw + 2, ny = th + 2;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = 1 + p % nx, ly = 1 + p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          const long long q = I2(P, ring_i(rr0 + lx), j);
+          const double A = (S(F_TE, lx, ly) - S(F_TE, lx - 1, ly)) / ld(P.dxx[1], q);
+          const double B = (j >= 2) ? (S(F_TN, lx, ly) - S(F_TN, lx, ly - 1)) / ld(P.dxy[1], q) : 0.0;
+          const double div = (A + B) / (a * ld(P.rh[1], q));
+          double pred;
+          if (__ldg(P.lev_t + q) > 0) pred = S(F_CH, lx, ly) - div * bt * gamma_b / ld(P.prh_t, q);
+          else pred = land_ch[q];
+          S(F_PRED, lx, ly) = pred;
+        }
+      }
+      __syncthreads();
+      // --- S5: sch_e on U [1, tw+2) x [1, th+2); N-grid values on [1, tw+3) x [1, th+2);
+      //         E-grid values on [1, tw+2) x [1, th+3)
+      {
+        const int nx = tw + 2, ny = th + 2;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = 1 + p % nx, ly = 1 + p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          const long long q = I2(P, ring_i(rr0 + lx), j);
+          const bool nrow = j <= njm, srow = j >= 2;
+          // U: sch_e
+          if (lx < tw + 2 && ly < th + 2) {
+            double sch = 1.0;
+            if (__ldg(P.lev_u + q) > 0) {
+              const double w = nrow ? (S(F_PRED, lx, ly) + S(F_PRED, lx, ly + 1) + S(F_PRED, lx + 1, ly) +
+                                       S(F_PRED, lx + 1, ly + 1)) * 0.25
+                                    : 0.0;
+              sch = sqrt(w);
+            }
+            S(F_SCHE, lx, ly) = sch;
+          }
+          // N grid (i, j): a1 = p1(ub)/rh4, gy = gra_y(pred), cN = ter_N(pred)
+          if (ly < th + 2) {
+            const double dx4 = ld(P.dxx[4], q), rh4 = ld(P.rh[4], q);
+            S(F_A1U, lx, ly) = ((S(F_UB, lx, ly) - S(F_UB, lx - 1, ly)) / dx4) / rh4;
+            S(F_A1V, lx, ly) = ((S(F_VB, lx, ly) - S(F_VB, lx - 1, ly)) / dx4) / rh4;
+            if (nrow) {
+              S(F_GY, lx, ly) = ((S(F_PRED, lx, ly + 1) - S(F_PRED, lx, ly)) / ld(P.dxy[4], q)) / a;
+              S(F_CN, lx, ly) = 0.5 * (S(F_PRED, lx, ly) + S(F_PRED, lx, ly + 1));
+            } else {
+              S(F_GY, lx, ly) = 0.0;
+              S(F_CN, lx, ly) = 0.0;
+            }
+          }
+          // E grid (i, j): a2 = p2(ub)*rh2, gx = gra_x(pred), cE = ter_E(pred)
+          if (lx < tw + 2) {
+            const double rh2 = ld(P.rh[2], q);
+            if (srow) {
+              const double dy2 = ld(P.dxy[2], q);
+              S(F_A2U, lx, ly) = ((S(F_UB, lx, ly) - S(F_UB, lx, ly - 1)) / dy2) * rh2;
+              S(F_A2V, lx, ly) = ((S(F_VB, lx, ly) - S(F_VB, lx, ly - 1)) / dy2) * rh2;
+            } else {
+              S(F_A2U, lx, ly) = 0.0;
+              S(F_A2V, lx, ly) = 0.0;
+            }
+            S(F_GX, lx, ly) = ((S(F_PRED, lx + 1, ly) - S(F_PRED, lx, ly)) / ld(P.dxx[2], q)) / (a * rh2);
+            S(F_CE, lx, ly) = 0.5 * (S(F_PRED, lx, ly) + S(F_PRED, lx + 1, ly));
+          }
+        }
+      }
+      __syncthreads();
+      // --- S6: corrector velocity on U [1, tw+2) x [1, th+2)
+      {
+        const int nx = tw + 1, ny = th + 1;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = 1 + p % nx, ly = 1 + p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          const int i = ring_i(rr0 + lx);
+          const long long q = I2(P, i, j);
+          const bool nrow = j <= njm;
+          const double seau = (double)(__ldg(P.lev_u + q) >= 1);
+          const double rh3 = ld(P.rh[3], q), dx3 = ld(P.dxx[3], q), dy3 = ld(P.dxy[3], q);
+          const double aarh = a * a * rh3;
+          // op_lap (mod_op.f90:904-925)
+          const double L1u = (S(F_A1U, lx + 1, ly) - S(F_A1U, lx, ly)) / dx3;
+          const double L1v = (S(F_A1V, lx + 1, ly) - S(F_A1V, lx, ly)) / dx3;
+          const double L2u = nrow ? (S(F_A2U, lx, ly + 1) - S(F_A2U, lx, ly)) / dy3 : 0.0;
+          const double L2v = nrow ? (S(F_A2V, lx, ly + 1) - S(F_A2V, lx, ly)) / dy3 : 0.0;
+          const double am1 = ld(P.am, q);
+          const double vsu = seau * am1 * ((L1u + L2u) / aarh);
+          const double vsv = seau * am1 * ((L1v + L2v) / aarh);
+          double dvu, dvv;
+          if (nt == 1) {
+            dvu = vsu - vsu;
+            dvv = vsv - vsv;
+          } else {
+            dvu = vsu - VS0U[q];
+            dvv = vsv - VS0V[q];
+          }
+          // bottom-pressure gradient forces (mod_int.f90:211-233)
+          double gi1 = 0.0, cg1 = 0.0;
+          if (nrow) {
+            gi1 = 0.5 * (S(F_GX, lx, ly) * ld(P.bphi[0], q) + S(F_GX, lx, ly + 1) * ld(P.bphi[1], q + ni));
+            cg1 = 0.5 * (S(F_CE, lx, ly) * ld(P.bgra[0], q) + S(F_CE, lx, ly + 1) * ld(P.bgra[1], q + ni));
+          }
+          const double gi2 = 0.5 * (S(F_GY, lx, ly) * ld(P.bphi[2], q) + S(F_GY, lx + 1, ly) * ld(P.bphi[3], q + 1));
+          const double cg2 = 0.5 * (S(F_CN, lx, ly) * ld(P.bgra[2], q) + S(F_CN, lx + 1, ly) * ld(P.bgra[3], q + 1));
+          const double sch = S(F_SCHE, lx, ly);
+          const double pg1 = (gi1 + cg1 + ld(P.graphihx, q)) * seau * sch;
+          const double pg2 = (gi2 + cg2 + ld(P.graphihy, q)) * seau * sch;
+          const double cor = ld(P.cor, q), ut = ld(P.ut, q), vt = ld(P.vt, q);
+          const double ubp = S(F_UB, lx, ly), vbp = S(F_VB, lx, ly);
+          double p1 = seau * (dvu + ut - pg1 + 0.5 * cor * vbp);
+          double p2 = seau * (dvv + vt - pg2 - 0.5 * cor * ubp);
+          const double w1 = p1 * bt + ubp, w2 = p2 * bt + vbp;
+          const double cb = 0.5 * cor * bt;
+          double u1 = (w1 + 0.5 * cor * bt * w2) / (1 + cb * cb);
+          double v1 = (w2 - 0.5 * cor * bt * w1) / (1 + cb * cb);
+          u1 = 0.5 * (u1 + ubp);
+          v1 = 0.5 * (v1 + vbp);
+          p1 = seau * (dvu - pg1 + ut + cor * v1);
+          p2 = seau * (dvv - pg2 + vt - cor * u1);
+          const double ubc = p1 * bt + ubp, vbc = p2 * bt + vbp;
+          S(F_UBC, lx, ly) = ubc;
+          S(F_VBC, lx, ly) = vbc;
+          const double ps = ld(P.prh_u, q) * sch;
+          S(F_S1N, lx, ly) = ps * ubc;
+          S(F_X2N, lx, ly) = ps * vbc * rh3;
+          // the first substep's viscosity is kept for the later ones (mod_int.f90:202-207)
+          if (nt == 1 && lx >= 2 && ly >= 2) {
+            VS0U[q] = vsu;
+            VS0V[q] = vsv;
+          }
+        }
+      }
+      __syncthreads();
+      // --- S7: ter to E on [1, tw+2) x [2, th+2), ter to N on [2, tw+2) x [1, th+2)
+      {
+        const int nx = tw + 1, ny = th + 1;
+        for (int p = tid; p < nx * ny; p += nth) {
+          const int lx = 1 + p % nx, ly = 1 + p / nx;
+          const int j = jj0 + ly;
+          if (j < 1 || j > nj) continue;
+          if (ly >= 2) S(F_TEN, lx, ly) = (j >= 2) ? 0.5 * (S(F_S1N, lx, ly - 1) + S(F_S1N, lx, ly)) : 0.0;
+          if (lx >= 2) S(F_TNN, lx, ly) = 0.5 * (S(F_X2N, lx - 1, ly) + S(F_X2N, lx, ly));
+        }
+      }
+      __syncthreads();
+      // --- S8: corrector ch on the tile, store, accumulate
+      for (int p = tid; p < tw * th; p += nth) {
+        const int lx = 2 + p % tw, ly = 2 + p / tw;
+        const int j = jj0 + ly;
+        const int i = ring_i(rr0 + lx);
+        const long long q = I2(P, i, j);
+        const double A = (S(F_TEN, lx, ly) - S(F_TEN, lx - 1, ly)) / ld(P.dxx[1], q);
+        const double B = (j >= 2) ? (S(F_TNN, lx, ly) - S(F_TNN, lx, ly - 1)) / ld(P.dxy[1], q) : 0.0;
+        const double div = (A + B) / (a * ld(P.rh[1], q));
+        const double m1 = (double)(__ldg(P.lev_t + q) >= 1);
+        const double chn = S(F_CH, lx, ly) - m1 * div * bt / ld(P.prh_t, q);
+        const double ubc = S(F_UBC, lx, ly), vbc = S(F_VBC, lx, ly);
+        st2(dst_ch, P, i, q, chn);
+        st2(dst_ub, P, i, q, ubc);
+        st2(dst_vb, P, i, q, vbc);
+        if (nt <= nstep / 2) A_mch[q] = A_mch[q] + chn;
+        A_mch2[q] = A_mch2[q] + chn;
+        A_ua[q] = A_ua[q] + ubc;
+        A_va[q] = A_va[q] + vbc;
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(P, nblocks)) return;
+  }
+
+  // averages (mod_int.f90:276-288)
+  for (int t = blockIdx.x; t < ntiles; t += nblocks) {
+    const int tx = t % ntx, ty = t / ntx;
+    const int R0 = tx * TX, J0 = ty * TY + 1;
+    const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+    for (int p = tid; p < tw * th; p += nth) {
+      const int i = R0 + (p % tw) + 2, j = J0 + p / tw;
+      const long long q = I2(P, i, j);
+      const double ub = A_ua[q] / (nstep + 1), vb = A_va[q] / (nstep + 1);
+      const double mch = A_mch[q] / (nstep / 2 + 1), mch2 = A_mch2[q] / (nstep + 1);
+      st2(P.ubc, P, i, q, ub);
+      st2(P.vbc, P, i, q, vb);
+      st2(P.ubp, P, i, q, ub);
+      st2(P.vbp, P, i, q, vb);
+      st2(P.mch, P, i, q, mch);
+      st2(P.mch2, P, i, q, mch2);
+      st2(P.chc, P, i, q, mch2);
+      st2(P.chp, P, i, q, mch2);
+      st2(P.acch, P, i, q, P.acch[q] + mch2);
+    }
+  }
+}
+
+size_t trop_smem_bytes(int TX, int TY) { return (size_t)F_COUNT * (TX + 4) * (TY + 4) * sizeof(double); }
+
+cudaError_t launch_trop(const Dev &P, int TX, int TY, int nblocks, cudaStream_t s) {
+  const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
+  const size_t smem = trop_smem_bytes(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(k_trop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&nty};
+  return cudaLaunchCooperativeKernel((const void *)k_trop, dim3(nblocks), dim3(256), args, smem, s);
+}
+
+int trop_max_blocks(int TX, int TY) {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = trop_smem_bytes(TX, TY);
+  cudaFuncSetAttribute(k_trop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop, 256, smem);
+  return per * nsm;
+}

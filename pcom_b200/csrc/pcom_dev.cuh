@@ -1,0 +1,134 @@
+// pcom_dev.cuh -- device-side view of one PCOM domain and the helpers every
+// kernel shares.
+//
+// Layout in HBM: every field is FP64, Fortran order (i fastest) over the
+// padded ni x nj domain, one contiguous plane per level.  The two x-halo
+// columns (1 and ni) of every stored field hold copies of columns ni-1 and 2:
+// that is what the reference's halo exchange leaves behind after each
+// operator with npx = 1 (mod_mympi.f90:669-746), and because every operator
+// covers all interior columns, every field the reference computes is
+// periodic over the glo_ni interior columns.  Kernels therefore compute the
+// interior columns 2..ni-1 with ring neighbours and also store the halo twin.
+// Rows 1 and nj are NOT exchanged (MPI_PROC_NULL, mod_param.f90:299-305):
+// each operator's row range and default value is reproduced explicitly.
+//
+// Arithmetic: the FP64 path is compiled with --fmad=false and keeps the
+// reference's evaluation order, so results are bitwise those of the
+// reference's gfortran build on x86-64 (SSE2, no FMA).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define PCOM_MAXK 64
+
+struct DevConsts {
+  double g, a, a0, rho0, pi, gamma_t, gamma_s, gamma_b, deltat, deltas, cdbot, tice, smag_c, ah_c;
+  double c_tc, c_tp, c_tpp;
+  double eos[42];
+};
+
+// Everything a kernel needs, passed by value as a __grid_constant__ param.
+struct Dev {
+  int ni, nj, nk, nkp, nim, njm, glo_ni, glo_nj;
+  int bt, bc, nstep, rst;
+  long long n2, n3, n3p;
+  DevConsts c;
+  double pr2[PCOM_MAXK], dpr2[PCOM_MAXK], dz1[PCOM_MAXK + 1];  // 1-based: [k]
+  // static 2D (index 1..4 = grid g1j..g4j)
+  const double *rh[5], *dxx[5], *dxy[5];
+  const double *tn3;
+  const int *lev_t, *lev_u;
+  const double *prh_t, *phih_t, *prh_u;
+  const double *cv1, *cv2, *cor, *graphihx, *graphihy;
+  const double *km, *kh;  // nkp levels
+  // forcing (bnd)
+  const double *taux, *tauy, *bnd_t, *bnd_s, *bnd_pa;
+  // state
+  double *tc, *sc, *tp, *sp;
+  double *uc, *vc, *up, *vp;
+  double *auc, *aup, *aupp, *avc, *avp, *avpp;
+  double *ubc, *vbc, *ubp, *vbp;
+  double *chc, *chp, *mch, *mch2;
+  double *am, *alpha, *adp, *wm;
+  double2 *prho;
+  // step intermediates
+  double *fx, *fy, *pax, *pay, *ut, *vt;
+  double *bphi[4], *bgra[4];  // xn, xs, ye, yw
+  double *sch_r, *sch_w;      // readyc sch (land 1) and upwelling sqrt(ter(chp))
+  double *uu, *vv;            // unweighted velocity for smag
+  double *tn_, *sn_;          // new T/S (int_ts writes here, then pointers rotate)
+  // accumulators
+  double *act, *acs, *acr, *acu, *acv, *acw, *acch, *acssh;
+  // barotropic subcycle scratch
+  double *tr_ch[2], *tr_ub[2], *tr_vb[2];
+  double *tr_acc[6];  // mch, mch2, ub, vb accumulators; first-substep viscosity (u, v)
+  unsigned *bar;   // [0] arrival count, [1] generation
+  int *err;        // [0] timeout flag, [1] watchdog flag
+  // AB3 start-up control for the current step
+  int ab3_mode;    // 0 normal, 1 step 1 (copy auc into aup, aupp), 2 step 2 (aupp = aup)
+};
+
+#define PD __device__ __forceinline__
+
+PD long long I2(const Dev &P, int i, int j) { return (long long)(i - 1) + (long long)P.ni * (j - 1); }
+PD long long I3(const Dev &P, int i, int j, int k) { return I2(P, i, j) + P.n2 * (k - 1); }
+// ring neighbours of an interior column (2 <= i <= ni-1)
+PD int IM(const Dev &P, int i) { return i == 2 ? P.ni - 1 : i - 1; }
+PD int IP(const Dev &P, int i) { return i == P.ni - 1 ? 2 : i + 1; }
+
+PD double ld(const double *p, long long q) { return __ldg(p + q); }
+
+// store to an interior column and to its halo twin
+PD void st2(double *p, const Dev &P, int i, long long q, double v) {
+  p[q] = v;
+  if (i == 2) p[q + (P.ni - 2)] = v;
+  else if (i == P.ni - 1) p[q - (P.ni - 2)] = v;
+}
+
+// den_rho, mod_den.f90:57-118, same evaluation order as the reference.
+PD double den_rho(const DevConsts &C, double t, double s, double p0) {
+  const double *e = C.eos;
+  double p = p0 * e[41];
+  double p2 = p * p;
+  double t2 = t * t;
+  double t3 = t2 * t;
+  double t4 = t3 * t;
+  double t5 = t4 * t;
+  double s32 = s * sqrt(s);
+  double s2 = s * s;
+  double r0 = e[0] + e[1] * t - e[2] * t2 + e[3] * t3 - e[4] * t4 + e[5] * t5;
+  double a = e[6] - e[7] * t + e[8] * t2 - e[9] * t3 + e[10] * t4;
+  double b = -e[11] + e[12] * t - e[13] * t2;
+  double r = r0 + a * s + b * s32 + e[14] * s2;
+  double k = e[15] + e[16] * t - e[17] * t2 + e[18] * t3 - e[19] * t4 +
+             (e[20] - e[21] * t + e[22] * t2 - e[23] * t3) * s +
+             (e[24] + e[25] * t - e[26] * t2) * s32 +
+             (e[27] + e[28] * t - e[29] * t2 + e[30] * t3) * p +
+             (e[31] - e[32] * t + e[33] * t2) * s * p + e[34] * s32 * p +
+             (e[35] - e[36] * t + e[37] * t2) * p2 +
+             (-e[38] + e[39] * t + e[40] * t2) * s * p2;
+  return r / (1.0 - p / k);
+}
+
+// ---------------------------------------------------------------------------
+// 2-D staggered-grid primitives.  Grids: T = g1j, E = g2j, U = g3j, N = g4j
+// (mod_arrays.f90:148-166).  Each helper returns the value the reference's
+// operator leaves at (i, j) after its halo exchange; i must be interior.
+
+// ter T->U, diagonal 4-point mean (ter_r2d, hga = g1j, mod_op.f90:416-419);
+// rows j = nj get the default `dft`.
+PD double terTU(const Dev &P, const double *f, int i, int j, double dft) {
+  if (j > P.njm) return dft;
+  long long q = I2(P, i, j);
+  return (ld(f, q) + ld(f, q + P.ni) + ld(f, q + 1) + ld(f, q + 1 + P.ni)) * 0.25;
+}
+
+// msk of the T grid (g12) and U grid (g32): set_grid builds msk = (lev >= k)
+// (main.f90:605-625); pcom_gpu_upload_static checks that the given masks are
+// exactly that, so kernels derive them from the 2-D lev arrays.
+PD double mT(const Dev &P, long long q2, int k) { return (double)(__ldg(P.lev_t + q2) >= k); }
+PD double mU(const Dev &P, long long q2, int k) { return (double)(__ldg(P.lev_u + q2) >= k); }
+
+// launch geometry shared by the column kernels
+#define COLS_X 32
+#define COLS_Y 4

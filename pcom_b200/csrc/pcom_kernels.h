@@ -1,0 +1,24 @@
+// pcom_kernels.h -- launchers of the device kernels (internal to libpcomgpu).
+#pragma once
+#include <cuda_runtime.h>
+#include "pcom_dev.cuh"
+
+void launch_alpha_tobot(const Dev &P, cudaStream_t s);
+void launch_pgra2d(const Dev &P, cudaStream_t s);
+void launch_uv2d(const Dev &P, int mode, cudaStream_t s);
+void launch_upwelling(const Dev &P, int with_acw, cudaStream_t s);
+void launch_readyc3d(const Dev &P, cudaStream_t s);
+void launch_clin(const Dev &P, cudaStream_t s);
+void launch_smag(const Dev &P, cudaStream_t s);
+void launch_ssh(const Dev &P, cudaStream_t s);
+void launch_ts(const Dev &P, cudaStream_t s);
+void launch_den_prho(const Dev &P, cudaStream_t s);
+
+size_t trop_smem_bytes(int TX, int TY);
+cudaError_t launch_trop(const Dev &P, int TX, int TY, int nblocks, cudaStream_t s);
+int trop_max_blocks(int TX, int TY);
+
+// watchdog: count non-finite values of a field over wet points of the T or U
+// grid (mask from lev), atomically added into *count
+void launch_nonfinite(const double *f, const int *lev, int nk, long long n2, int planes, unsigned long long *count,
+                      cudaStream_t s);
