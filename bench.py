@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark: simulated years per wall-clock day (SYPD) of the PCOM baroclinic
+step at 1 degree x 30 levels (360 x 160 x 30 near-global synthetic case) on
+B200, FP64 plain path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one baroclinic step of dtbc = 3600 s (main.f90:205-223: EOS,
+pressure-gradient integrals, advection/friction, the 120-substep barotropic
+subcycle, baroclinic momentum, SSH, tracers with convective adjustment), plus
+the daily density derivatives when the model day changes.  SYPD =
+(steps * 3600 s / 365 d) / wall days.  With N > 1 GPUs every rank advances its
+own ensemble member (replicas, no data-path collective): value = the sum over
+ranks, timed as the max over ranks.
+
+--impl reference times the reference algorithm's CPU implementation (the C++
+restatement in oracle/, OpenMP over all host cores) on the same case.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CASE = "global1"
+STEP_SECONDS = 3600
+YEAR_STEPS = 365 * 86400 / STEP_SECONDS  # 8760 steps per model year
+
+
+def sypd(seconds_per_step: float) -> float:
+    return (86400.0 / seconds_per_step) / YEAR_STEPS
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=48)
+    p.add_argument("--warmup", type=int, default=4)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-sample-steps", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- roofline
+def algorithmic_bytes(kernel: str, glo_ni: int, glo_nj: int, nk: int, nstep: int) -> float:
+    """Bytes a kernel must move per launch at minimum (FP64, wet or not).
+
+    3-D fields count glo_ni*glo_nj*nk points, 2-D fields glo_ni*glo_nj.  The
+    per-kernel field counts are the reads/writes listed in DESIGN.md."""
+    n2 = glo_ni * glo_nj
+    n3 = n2 * nk
+    s = 8.0
+    table = {
+        # kernel: (3-D fields read+written, 2-D fields read+written)
+        "den_alpha+int_tobot": (4, 1),         # R tc, sc; W alpha, adp; R chc
+        "int_pgra": (2, 8 + 4),                # R alpha, adp; W bphi/bgraphi (8); statics
+        "readyc_2d": (0, 4 + 6),
+        "upwelling": (3, 4),                   # R uc, vc; W wm
+        "readyc_3d": (2 + 1 + 2 + 4 + 1, 6),   # R uc, vc, wm, am, (km); W auc, avc, fx, fy
+        "int_trop": (0, nstep * 6 + 30),       # per substep R/W ch, ub, vb; statics once
+        "int_clin": (12 + 7, 8),               # R adp, alpha, 6 AB3, fx, fy, uc, vc, up, vp; W uc, vc, up, vp, uu, vv, acu
+        "smag": (3, 2),
+        "int_ssh": (3, 3),
+        "ts_2d": (0, 4),
+        "upwelling+acw": (6, 4),
+        "int_ts": (4 + 2 + 1 + 2 + 1 + 2 + 6, 6),  # R tc, sc, tp, sp, uc, vc, wm, kh, prho(2); W tn, sn; RW act, acs, acr
+        "den_prho": (4, 1),
+    }
+    f3, f2 = table.get(kernel, (0, 0))
+    return s * (f3 * n3 + f2 * n2)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from pcom_b200 import _lib as L
+    from pcom_b200.model import Model
+    from pcom_b200.synth import make_case, perturb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    case = make_case(CASE)
+    if world > 1 and rank > 0:
+        case = perturb(case, rank)  # each rank integrates its own ensemble member
+    m = Model(case)
+    stream = torch.cuda.current_stream()
+    m.set_stream(stream.cuda_stream)
+    lib, h = m.lib, m.handle
+    ni, nj, nk = m.ni, m.nj, m.nk
+    n2 = ni * nj
+
+    # warm-up through the host driver (includes the AB3 start-up steps)
+    m.run(max(args.warmup, 3))
+    it0 = m.iter
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ------------------------------------------------ value: device-resident
+    # per step: den_prho when the model day changes (every 24 steps), then the
+    # step block.  The state (~0.9 GB) is far larger than L2 (126 MB).
+    steps = args.steps
+    day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
+    m.profile(True)
+    launches0 = m.launch_count()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        for q in range(steps):
+            it = it0 + 1 + q
+            if day_of(it) != day_of(it - 1):
+                L.check(lib.pcom_gpu_den_prho(h), "den_prho")
+            L.check(lib.pcom_gpu_step_async(h, it), "step")
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1)
+    launches = m.launch_count() - launches0
+    prof = m.profile_read()
+    m.profile(False)
+    L.check(lib.pcom_gpu_check_finite(h), "watchdog")
+    t_max = t_ms
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    ms_per_step = t_max / steps
+    value = world * sypd(ms_per_step / 1000.0)
+
+    # ------------------------------------------------ e2e: host buffers
+    # per step through the reference-facing API: the day's forcing from pinned
+    # host memory (int_bnd on the host), the step, and the barotropic state
+    # (ch, ub, vb) read back into pinned host memory.
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True)
+    frc = [pin(n2) for _ in range(6)]
+    out = [pin(n2) for _ in range(3)]
+    host_f = m.int_bnd()
+    for t_, k_ in zip(frc, ("taux", "tauy", "t", "s", "pa", "fw")):
+        t_.copy_(torch.from_numpy(host_f[k_].reshape(-1)))
+    import ctypes as C
+    dp = lambda t_: C.cast(t_.data_ptr(), L.dbl_p)
+    fo = L.Forcing(*[dp(t_) for t_ in frc])
+    st_out = L.State(*[None] * len(L.STATE_FIELDS))
+    st_out.chc, st_out.ubc, st_out.vbc = dp(out[0]), dp(out[1]), dp(out[2])
+    it1 = it0 + steps
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for q in range(steps):
+        it = it1 + 1 + q
+        L.check(lib.pcom_gpu_set_forcing(h, C.byref(fo)), "set_forcing")
+        if day_of(it) != day_of(it - 1):
+            L.check(lib.pcom_gpu_den_prho(h), "den_prho")
+        L.check(lib.pcom_gpu_step(h, it), "step")
+        L.check(lib.pcom_gpu_get_state(h, C.byref(st_out)), "get_state")
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = world * sypd(e2e_ms / steps / 1000.0)
+
+    # ------------------------------------------------ roofline of the dominant kernel
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    top = max(prof.items(), key=lambda kv: kv[1][1]) if prof else ("", (1, 0.0))
+    kname, (klaunch, kms) = top
+    nstep = case["dtbc"] // case["dtbt"] * 2
+    kbytes = algorithmic_bytes(kname, case["glo_ni"], case["glo_nj"], nk, nstep)
+    avg_s = kms / max(klaunch, 1) / 1000.0
+    achieved = kbytes / avg_s / 1e9 if avg_s > 0 else 0.0
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+        traffic = tr.get(kname, {}).get("bytes_per_launch")
+    except Exception:
+        pass
+    kernels = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(x[1] for x in prof.values())), 4)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    # ------------------------------------------------ CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample_steps)
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": "SYPD at 1deg x 30L (360x160x30 near-global), FP64 plain path",
+            "value": round(value, 2),
+            "unit": "SYPD",
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring)",
+            "config": {
+                "workload": "global1: 360x160x30 1-degree near-global ocean, dtbc 3600 s, dtbt 60 s "
+                            "(120 barotropic substeps per step), one baroclinic step per step",
+                "grid": [case["glo_ni"], case["glo_nj"], nk],
+                "parallelism": "replicas" if world > 1 else "single GPU",
+                "l2": "inputs larger than L2: ~0.9 GB of resident state vs 126 MB L2",
+                "timing": "CUDA events on the model's stream; per-kernel events on in the timed region",
+            },
+            "e2e": {"value": round(e2e, 2), "unit": "SYPD", "h2d_bytes_per_step": 6 * n2 * 8,
+                    "d2h_bytes_per_step": 3 * n2 * 8},
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": round(achieved, 1),
+                         "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_launch": kbytes},
+            "kernels": kernels,
+            "gpu_launches": int(launches),
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    m.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(nsteps: int):
+    """The oracle (C++ restatement, OpenMP over all host threads) on a bounded
+    sample of the same workload: nsteps steps of the 360x160x30 case."""
+    from oracle import pyoracle
+    from pcom_b200.synth import make_case
+
+    threads = os.cpu_count() or 1
+    o = pyoracle.Oracle(make_case(CASE), threads=threads)
+    o.step(1)  # first step includes the AB3 start-up and the first den_prho
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    dt = (time.perf_counter() - t0) / nsteps
+    return {"value": round(sypd(dt), 3), "unit": "SYPD", "cores": threads, "kind": "port",
+            "sample": f"{nsteps} steps of the 360x160x30 case after 1 warm-up step, {dt:.3f} s/step"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    from pcom_b200.synth import make_case
+
+    threads = os.cpu_count() or 1
+    o = pyoracle.Oracle(make_case(CASE), threads=threads)
+    warm = max(1, min(args.warmup, 2))
+    o.step(warm)
+    # each timed step is one full baroclinic step; the sample is bounded so the
+    # run ends within minutes even for large --steps
+    nsteps = max(1, min(args.steps, 4))
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    dt = (time.perf_counter() - t0) / nsteps
+    v = sypd(dt)
+    line = {
+        "impl": "reference",
+        "metric": "SYPD at 1deg x 30L (360x160x30 near-global), FP64 plain path",
+        "value": round(v, 3), "unit": "SYPD", "n_gpus": world, "steps": nsteps, "warmup": warm,
+        "ms_per_step": round(dt * 1000, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring)",
+        "config": {"workload": "global1: 360x160x30 1-degree near-global ocean, dtbc 3600 s, dtbt 60 s",
+                   "grid": [360, 160, 30], "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "SYPD", "cores": threads, "kind": "port",
+                         "sample": f"{nsteps} steps after {warm} warm-up steps"},
+        "e2e": {"value": round(v, 3), "unit": "SYPD", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
