@@ -64,6 +64,11 @@ struct Dev {
   double *tr_acc[6];  // mch, mch2, ub, vb accumulators; first-substep viscosity (u, v)
   unsigned *bar;   // [0] arrival count, [1] generation
   int *err;        // [0] timeout flag, [1] watchdog flag
+  // lat-lon (separable) metrics: dx?x depends on i only, dx?y and rh? on j
+  // only (set_hgrid builds them from 1-D lon/lat, main.f90:408-493); when the
+  // uploaded 2-D arrays have that structure these 1-D copies are set
+  int separable;
+  const double *dxx1d[5], *dxy1d[5], *rh1d[5];  // [g][i-1] and [g][j-1]
   // AB3 start-up control for the current step
   int ab3_mode;    // 0 normal, 1 step 1 (copy auc into aup, aupp), 2 step 2 (aupp = aup)
 };

@@ -132,6 +132,7 @@ struct pcom_handle {
   bool static_ok = false;
   int n_ts = 0, n_uv = 0, n_w = 0, n_ch = 0, n_ssh = 0;
   int trop_tx = 24, trop_ty = 18, trop_blocks = 0;
+  bool trop_resident = false;
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
   long long launches = 0;
@@ -200,6 +201,27 @@ void bind_rotating(pcom_handle *h) {
 }
 
 int pick_trop_config(pcom_handle *h) {
+  // resident kernel: one tile per CTA, one region point per thread; pick the
+  // tiling with the fewest tiles (fewest CTAs at the grid barrier)
+  h->trop_resident = false;
+  if (h->D.separable) {
+    int best_n = 1 << 30, bx = 0, by = 0;
+    const int mb = trop_res_max_blocks(24, 18);
+    for (int ty = 6; ty <= 40; ++ty)
+      for (int tx = 6; tx <= 60; ++tx) {
+        if (!trop_res_fits(tx, ty)) continue;
+        const int nt = ((h->dims.glo_ni + tx - 1) / tx) * ((h->nj + ty - 1) / ty);
+        if (nt > mb) continue;
+        if (nt < best_n || (nt == best_n && (tx + 4) * (ty + 4) < (bx + 4) * (by + 4))) { best_n = nt; bx = tx; by = ty; }
+      }
+    if (bx > 0 && trop_res_max_blocks(bx, by) >= best_n) {
+      h->trop_resident = true;
+      h->trop_tx = bx;
+      h->trop_ty = by;
+      h->trop_blocks = best_n;
+      return PCOM_OK;
+    }
+  }
   // largest co-resident grid for the candidate tiles; prefer a tiling with at
   // most one tile per CTA (the whole subcycle then stays one wave)
   static const int cand[][2] = {{24, 18}, {32, 16}, {32, 24}, {32, 32}, {48, 32}, {64, 32}};
@@ -263,7 +285,8 @@ int do_trop(pcom_handle *h) {
     if (rc) return rc;
   }
   Prof p(h, "int_trop");
-  cudaError_t e = launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
+  cudaError_t e = h->trop_resident ? launch_trop_res(h->D, h->trop_tx, h->trop_ty, h->stream)
+                                   : launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "barotropic kernel launch: %s", cudaGetErrorString(e));
   h->n_ch++;
   return PCOM_OK;
@@ -425,6 +448,11 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
     D.rh[g] = r; D.dxx[g] = x; D.dxy[g] = y;
   }
   double *tn3; A(&tn3, n2); D.tn3 = tn3;
+  for (int g = 1; g <= 4; ++g) {
+    double *x, *y, *r;
+    A(&x, d.ni); A(&y, d.nj); A(&r, d.nj);
+    D.dxx1d[g] = x; D.dxy1d[g] = y; D.rh1d[g] = r;
+  }
   int *lt = nullptr, *lu = nullptr;
   if (!rc) rc = h->alloc(&lt, (size_t)n2);
   if (!rc) rc = h->alloc(&lu, (size_t)n2);
@@ -509,6 +537,28 @@ int pcom_gpu_upload_static(pcom_handle *h, const pcom_static *s) {
     CK(cudaMemcpy((void *)D.rh[g], s->rh[g - 1], n2 * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void *)D.dxx[g], bx.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void *)D.dxy[g], by.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  // lat-lon metrics: dx?x(i, j) = dx?x(i), dx?y(i, j) = dx?y(j), rh?(i, j) = rh?(j)
+  {
+    bool sep = true;
+    std::vector<double> x1((size_t)ni), y1((size_t)nj), r1((size_t)nj);
+    for (int g = 1; g <= 4 && sep; ++g) {
+      const double *dx = s->dx[g - 1], *rh = s->rh[g - 1];
+      for (int j = 0; j < nj && sep; ++j)
+        for (int i = 0; i < ni; ++i) {
+          const long long q = i + (long long)ni * j;
+          if (dx[2 * q] != dx[2 * (long long)i] || dx[2 * q + 1] != dx[2 * ((long long)ni * j) + 1] ||
+              rh[q] != rh[(long long)ni * j]) { sep = false; break; }
+        }
+      if (!sep) break;
+      for (int i = 0; i < ni; ++i) x1[i] = dx[2 * (long long)i];
+      for (int j = 0; j < nj; ++j) { y1[j] = dx[2 * ((long long)ni * j) + 1]; r1[j] = rh[(long long)ni * j]; }
+      CK(cudaMemcpy((void *)D.dxx1d[g], x1.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy((void *)D.dxy1d[g], y1.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy((void *)D.rh1d[g], r1.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    D.separable = sep ? 1 : 0;
+    h->trop_blocks = 0;  // re-pick the barotropic kernel configuration
   }
   if (!s->tn[2]) return fail(PCOM_ERR_ARG, "tn of grid 3 missing");
   CK(cudaMemcpy((void *)D.tn3, s->tn[2], n2 * sizeof(double), cudaMemcpyHostToDevice));

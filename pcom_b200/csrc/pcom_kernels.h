@@ -17,6 +17,11 @@ void launch_den_prho(const Dev &P, cudaStream_t s);
 size_t trop_smem_bytes(int TX, int TY);
 cudaError_t launch_trop(const Dev &P, int TX, int TY, int nblocks, cudaStream_t s);
 int trop_max_blocks(int TX, int TY);
+// resident variant: one tile per CTA, one region point per thread
+size_t trop_res_smem_bytes(int TX, int TY);
+bool trop_res_fits(int TX, int TY);
+cudaError_t launch_trop_res(const Dev &P, int TX, int TY, cudaStream_t s);
+int trop_res_max_blocks(int TX, int TY);
 
 // watchdog: count non-finite values of a field over wet points of the T or U
 // grid (mask from lev), atomically added into *count
