@@ -160,6 +160,33 @@ int pcom_gpu_profile_read(pcom_handle *h, char *names, int64_t *launches, double
 /* Number of this library's kernel launches issued so far on this handle. */
 int64_t pcom_gpu_launch_count(pcom_handle *h);
 
+/* --- allocation-free barotropic subcycle -------------------------------- */
+/* No counterpart in the reference.  One int_trop subcycle (the same kernel
+ * and arithmetic as pcom_gpu_step uses) over arrays the caller owns, for
+ * callers that must not allocate device memory: code running while a stream
+ * is being captured into a CUDA graph (cudaMalloc is not allowed there), and
+ * host frameworks that hand every byte of device memory out from their own
+ * pool.  All pointers are device pointers in Fortran order; FP64 fields are
+ * ni*nj (lev_* int32).  The metrics are given as separate components
+ * (dxx = dx%x(1), dxy = dx%x(2)) of grids 1..4.  am1 is am(:,:,1).
+ * The scratch this needs (halo ping-pong buffers, 1-D metric copies and the
+ * grid-barrier words) is a fixed array inside the library, sized for
+ * ni*nj <= PCOM_NOALLOC_MAX_POINTS and ni, nj <= PCOM_NOALLOC_MAX_DIM; larger
+ * domains are rejected with PCOM_ERR_ARG.  The first call on a device looks
+ * up that array's device address, so make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
+#define PCOM_NOALLOC_MAX_POINTS 65536
+#define PCOM_NOALLOC_MAX_DIM 1024
+typedef struct pcom_trop_io {
+  int32_t glo_ni, glo_nj, dtbt, dtbc, flags;   /* flags: PCOM_LIT_R8 or 0 */
+  const int32_t *lev_t, *lev_u;
+  const double *prh_t, *prh_u, *cor, *am1, *graphihx, *graphihy;
+  const double *dxx[4], *dxy[4], *rh[4];
+  const double *ut, *vt, *bphi[4], *bgraphi[4]; /* xn, xs, ye, yw */
+  double *chc, *chp, *mch, *mch2, *ubc, *vbc, *ubp, *vbp, *acch;
+} pcom_trop_io;
+int pcom_gpu_trop_noalloc(const pcom_trop_io *io, void *stream);
+
 /* Message of the last failed call on this thread. */
 int pcom_gpu_last_error(char *buf, int32_t len);
 

@@ -56,6 +56,18 @@ class Accum(C.Structure):
     _fields_ = [(n, dbl_p) for n in ACCUM_FIELDS] + [(n, C.c_int32) for n in ("n_ts", "n_uv", "n_w", "n_ch", "n_ssh")]
 
 
+class TropIO(C.Structure):
+    _fields_ = [("glo_ni", C.c_int32), ("glo_nj", C.c_int32), ("dtbt", C.c_int32), ("dtbc", C.c_int32),
+                ("flags", C.c_int32), ("lev_t", C.c_void_p), ("lev_u", C.c_void_p),
+                ("prh_t", C.c_void_p), ("prh_u", C.c_void_p), ("cor", C.c_void_p), ("am1", C.c_void_p),
+                ("graphihx", C.c_void_p), ("graphihy", C.c_void_p),
+                ("dxx", C.c_void_p * 4), ("dxy", C.c_void_p * 4), ("rh", C.c_void_p * 4),
+                ("ut", C.c_void_p), ("vt", C.c_void_p), ("bphi", C.c_void_p * 4), ("bgraphi", C.c_void_p * 4),
+                ("chc", C.c_void_p), ("chp", C.c_void_p), ("mch", C.c_void_p), ("mch2", C.c_void_p),
+                ("ubc", C.c_void_p), ("vbc", C.c_void_p), ("ubp", C.c_void_p), ("vbp", C.c_void_p),
+                ("acch", C.c_void_p)]
+
+
 class Case(C.Structure):
     _fields_ = [("glo_ni", C.c_int32), ("glo_nj", C.c_int32), ("nk", C.c_int32), ("dtbt", C.c_int32),
                 ("dtbc", C.c_int32), ("r8", C.c_int32), ("rst", C.c_int32), ("year", C.c_int32),
@@ -88,6 +100,7 @@ SIGNATURES = {
     "pcom_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64), dbl_p, C.c_int32]),
     "pcom_gpu_launch_count": (C.c_int64, [C.c_void_p]),
     "pcom_gpu_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
+    "pcom_gpu_trop_noalloc": (C.c_int, [C.POINTER(TropIO), C.c_void_p]),
     "pcom_model_create": (C.c_int, [C.POINTER(Case), C.c_int32, C.POINTER(C.c_void_p)]),
     "pcom_model_destroy": (C.c_int, [C.c_void_p]),
     "pcom_model_handle": (C.c_void_p, [C.c_void_p]),

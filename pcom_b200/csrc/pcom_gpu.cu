@@ -774,3 +774,9 @@ int pcom_gpu_profile_read(pcom_handle *h, char *names, int64_t *launches, double
 int64_t pcom_gpu_launch_count(pcom_handle *h) { return h ? h->launches : 0; }
 
 }  // extern "C"
+
+// constants of a handle, for entry points that build their own device view
+void pcom_dev_consts(bool r8, DevConsts &c) { make_consts(r8, c); }
+
+// record a failure for pcom_gpu_last_error from another translation unit
+int pcom_set_error(int code, const char *msg) { return fail(code, "%s", msg); }

@@ -23,6 +23,11 @@ bool trop_res_fits(int TX, int TY);
 cudaError_t launch_trop_res(const Dev &P, int TX, int TY, cudaStream_t s);
 int trop_res_max_blocks(int TX, int TY);
 
+// the model constants (literal precision per PCOM_LIT_R8)
+void pcom_dev_consts(bool r8, DevConsts &c);
+// set the message returned by pcom_gpu_last_error; returns code
+int pcom_set_error(int code, const char *msg);
+
 // watchdog: count non-finite values of a field over wet points of the T or U
 // grid (mask from lev), atomically added into *count
 void launch_nonfinite(const double *f, const int *lev, int nk, long long n2, int planes, unsigned long long *count,
