@@ -666,3 +666,285 @@ int trop_res_max_blocks(int TX, int TY) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_res, nthreads, smem) != cudaSuccess) return 0;
   return per * nsm;
 }
+
+// ============================================================================
+// Fast variant of the resident kernel: the same arithmetic with every division
+// by a static metric, bottom pressure or Coriolis denominator done with its
+// correctly rounded reciprocal (dvr), which removes the per-division
+// reciprocal-approximation instruction from the critical path.
+
+__global__ void __launch_bounds__(kResThreads, 1)
+    k_trop_fast(const __grid_constant__ Dev P, int TX, int TY, int ntx) {
+  extern __shared__ double sm[];
+  const int ni = P.ni, nj = P.nj, njm = P.njm, G = P.glo_ni;
+  const int W = TX + 4, H = TY + 4, RS = W * H;
+  double *vx = sm + R_COUNT * RS;  // dxx[1..4], 1/dxx[1..4] over lx: 8*W
+  double *vy = vx + 8 * W;         // kFastVy vectors over ly (see below)
+  const double a = P.c.a, bt = (double)P.bt, gamma_b = P.c.gamma_b;
+  const int nstep = P.nstep;
+  const unsigned nblocks = gridDim.x;
+  const int tid = threadIdx.x;
+  const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+  const int R0 = tx * TX, J0 = ty * TY + 1;
+  const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+  const int rr0 = R0 - 2, jj0 = J0 - 2;
+  auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
+
+  // 1-D metrics and the reciprocals of every divisor (dvr)
+  for (int l = tid; l < W; l += blockDim.x) {
+    const int i = ring_i(rr0 + l);
+    for (int g = 1; g <= 4; ++g) {
+      vx[(g - 1) * W + l] = ld(P.dxx1d[g], i - 1);
+      vx[(4 + g - 1) * W + l] = ld(P.rdxx1d[g], i - 1);
+    }
+  }
+  for (int l = tid; l < H; l += blockDim.x) {
+    const int j = jj0 + l;
+    if (j < 1 || j > nj) continue;
+    for (int g = 1; g <= 4; ++g) {
+      vy[(g - 1) * H + l] = ld(P.dxy1d[g], j - 1);
+      vy[(4 + g - 1) * H + l] = ld(P.rdxy1d[g], j - 1);
+      vy[(8 + g - 1) * H + l] = ld(P.rh1d[g], j - 1);
+    }
+    vy[12 * H + l] = ld(P.arh1d[1], j - 1);
+    vy[13 * H + l] = ld(P.rarh1d[1], j - 1);
+    vy[14 * H + l] = ld(P.arh1d[2], j - 1);
+    vy[15 * H + l] = ld(P.rarh1d[2], j - 1);
+    vy[16 * H + l] = ld(P.rrh1d[4], j - 1);
+    vy[17 * H + l] = ld(P.aarh3, j - 1);
+    vy[18 * H + l] = ld(P.raarh3, j - 1);
+  }
+  auto DXX = [&](int g, int lx) { return vx[(g - 1) * W + lx]; };
+  auto RDXX = [&](int g, int lx) { return vx[(4 + g - 1) * W + lx]; };
+  auto DXY = [&](int g, int ly) { return vy[(g - 1) * H + ly]; };
+  auto RDXY = [&](int g, int ly) { return vy[(4 + g - 1) * H + ly]; };
+  auto RH = [&](int g, int ly) { return vy[(8 + g - 1) * H + ly]; };
+  const double ra = P.ra;
+  auto S = [&](int f, int p) -> double & { return sm[f * RS + p]; };
+
+  // this thread's region point
+  const int p = tid;
+  const int lx = p % W, ly = p / W;
+  const int j = jj0 + ly;
+  const bool active = p < RS && j >= 1 && j <= nj;
+  const int i = active ? ring_i(rr0 + lx) : 2;
+  const long long q = active ? I2(P, i, j) : 0;
+  const bool nrow = j <= njm, srow = j >= 2;
+  const bool inS2 = active && lx < tw + 3 && ly < th + 3;
+  const bool inS4 = active && lx >= 1 && lx < tw + 3 && ly >= 1 && ly < th + 3;
+  const bool inS6 = active && lx >= 1 && lx < tw + 2 && ly >= 1 && ly < th + 2;
+  const bool inN = active && lx >= 1 && lx < tw + 3 && ly >= 1 && ly < th + 2;
+  const bool inE = active && lx >= 1 && lx < tw + 2 && ly >= 1 && ly < th + 3;
+  const bool inS8 = active && lx >= 2 && lx < tw + 2 && ly >= 2 && ly < th + 2;
+  const int levu = active ? __ldg(P.lev_u + q) : 0, levt = active ? __ldg(P.lev_t + q) : 0;
+  const double seau = (double)(levu >= 1), mskt1 = (double)(levt >= 1);
+  const double prh_u = active ? ld(P.prh_u, q) : 1.0, prh_t = active ? ld(P.prh_t, q) : 1.0;
+  const double rprh_t = active ? ld(P.rprh_t, q) : 1.0;
+  const double rden = active ? ld(P.rwt, q) : 1.0;  // 1 / (1 + (0.5 cor dtbt)^2)
+  // S6 coefficients (shifted where the reference's formulas shift them)
+  double sam1 = 0, bxn = 0, bxs = 0, bye = 0, byw = 0, gxn = 0, gxs = 0, gye = 0, gyw = 0;
+  double ghx = 0, ghy = 0, cor = 0, ut = 0, vt = 0;
+  if (inS6) {
+    sam1 = seau * ld(P.am, q);
+    bxn = ld(P.bphi[0], q); bye = ld(P.bphi[2], q); byw = ld(P.bphi[3], q + 1);
+    gxn = ld(P.bgra[0], q); gye = ld(P.bgra[2], q); gyw = ld(P.bgra[3], q + 1);
+    if (nrow) { bxs = ld(P.bphi[1], q + ni); gxs = ld(P.bgra[1], q + ni); }
+    ghx = ld(P.graphihx, q); ghy = ld(P.graphihy, q);
+    cor = ld(P.cor, q); ut = ld(P.ut, q); vt = ld(P.vt, q);
+  }
+  double vs0u = 0.0, vs0v = 0.0;
+  // accumulators (mod_int.f90:176-180)
+  double acc_m = 0, acc_m2 = 0, acc_u = 0, acc_v = 0;
+  if (inS8) {
+    acc_m = P.chc[q]; acc_m2 = acc_m;
+    acc_u = P.ubc[q]; acc_v = P.vbc[q];
+  }
+  const double land_ch0 = inS4 ? P.chc[q] : 0.0;
+  __syncthreads();
+
+  for (int nt = 1; nt <= nstep; ++nt) {
+    const int d = (nt - 1) & 1;
+    const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
+    const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
+    const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
+    // S1: previous state
+    if (active) {
+      S(R_CH, p) = src_ch[q];
+      if (inS2) { S(R_UB, p) = src_ub[q]; S(R_VB, p) = src_vb[q]; }
+    }
+    __syncthreads();
+    // S2: sch = sqrt(ter(ch)) on U, supb
+    if (inS2) {
+      double sch = 1.0;
+      if (levu > 0) {
+        const double w = nrow ? (S(R_CH, p) + S(R_CH, p + W) + S(R_CH, p + 1) + S(R_CH, p + W + 1)) * 0.25 : 0.0;
+        sch = sqrt(w);
+      }
+      const double ps = prh_u * sch;
+      S(R_S1, p) = ps * S(R_UB, p);
+      S(R_X2, p) = ps * S(R_VB, p) * RH(3, ly);
+    }
+    __syncthreads();
+    // S4: predictor ch; the ter U->E (rows >= 2) and U->N means of supb are
+    // formed here from the staged supb
+    if (inS4) {
+      // tE at (i, j) and (i-1, j): j >= 2 ? 0.5 (s1(j-1) + s1(j)) : 0
+      const double tEc = srow ? 0.5 * (S(R_S1, p - W) + S(R_S1, p)) : 0.0;
+      const double tEw = srow ? 0.5 * (S(R_S1, p - W - 1) + S(R_S1, p - 1)) : 0.0;
+      const double A = dvr(tEc - tEw, DXX(1, lx), RDXX(1, lx));
+      double B = 0.0;
+      if (srow) {
+        // tN at (i, j) and (i, j-1): 0.5 (x2(i-1) + x2(i))
+        const double tNc = 0.5 * (S(R_X2, p - 1) + S(R_X2, p));
+        const double tNs = 0.5 * (S(R_X2, p - W - 1) + S(R_X2, p - W));
+        B = dvr(tNc - tNs, DXY(1, ly), RDXY(1, ly));
+      }
+      const double div = dvr(A + B, vy[12 * H + ly], vy[13 * H + ly]);
+      double pred;
+      if (levt > 0) pred = S(R_CH, p) - dvr(div * bt * gamma_b, prh_t, rprh_t);
+      else pred = (nt == 1) ? land_ch0 : S(R_CH, p);
+      S(R_PRED, p) = pred;
+    }
+    __syncthreads();
+    // S5: sch on U; N- and E-grid intermediates
+    if (inS6) {
+      double sch = 1.0;
+      if (levu > 0) {
+        const double w = nrow ? (S(R_PRED, p) + S(R_PRED, p + W) + S(R_PRED, p + 1) + S(R_PRED, p + W + 1)) * 0.25 : 0.0;
+        sch = sqrt(w);
+      }
+      S(R_SCHE, p) = sch;
+    }
+    if (inN) {
+      const double dx4 = DXX(4, lx), rdx4 = RDXX(4, lx), rh4 = RH(4, ly), rrh4 = vy[16 * H + ly];
+      S(R_A1U, p) = dvr(dvr(S(R_UB, p) - S(R_UB, p - 1), dx4, rdx4), rh4, rrh4);
+      S(R_A1V, p) = dvr(dvr(S(R_VB, p) - S(R_VB, p - 1), dx4, rdx4), rh4, rrh4);
+      if (nrow) {
+        S(R_GY, p) = dvr(dvr(S(R_PRED, p + W) - S(R_PRED, p), DXY(4, ly), RDXY(4, ly)), a, ra);
+        S(R_CN, p) = 0.5 * (S(R_PRED, p) + S(R_PRED, p + W));
+      } else {
+        S(R_GY, p) = 0.0;
+        S(R_CN, p) = 0.0;
+      }
+    }
+    if (inE) {
+      const double rh2 = RH(2, ly);
+      if (srow) {
+        const double dy2 = DXY(2, ly), rdy2 = RDXY(2, ly);
+        S(R_A2U, p) = dvr(S(R_UB, p) - S(R_UB, p - W), dy2, rdy2) * rh2;
+        S(R_A2V, p) = dvr(S(R_VB, p) - S(R_VB, p - W), dy2, rdy2) * rh2;
+      } else {
+        S(R_A2U, p) = 0.0;
+        S(R_A2V, p) = 0.0;
+      }
+      S(R_GX, p) = dvr(dvr(S(R_PRED, p + 1) - S(R_PRED, p), DXX(2, lx), RDXX(2, lx)), vy[14 * H + ly], vy[15 * H + ly]);
+      S(R_CE, p) = 0.5 * (S(R_PRED, p) + S(R_PRED, p + 1));
+    }
+    __syncthreads();
+    // S6: corrector velocity (viscosity, pressure gradient, Coriolis adjustment)
+    if (inS6) {
+      const double rh3 = RH(3, ly), dx3 = DXX(3, lx), rdx3 = RDXX(3, lx), dy3 = DXY(3, ly), rdy3 = RDXY(3, ly);
+      const double aarh = vy[17 * H + ly], raarh = vy[18 * H + ly];
+      const double L1u = dvr(S(R_A1U, p + 1) - S(R_A1U, p), dx3, rdx3);
+      const double L1v = dvr(S(R_A1V, p + 1) - S(R_A1V, p), dx3, rdx3);
+      const double L2u = nrow ? dvr(S(R_A2U, p + W) - S(R_A2U, p), dy3, rdy3) : 0.0;
+      const double L2v = nrow ? dvr(S(R_A2V, p + W) - S(R_A2V, p), dy3, rdy3) : 0.0;
+      const double vsu = sam1 * dvr(L1u + L2u, aarh, raarh);
+      const double vsv = sam1 * dvr(L1v + L2v, aarh, raarh);
+      if (nt == 1) { vs0u = vsu; vs0v = vsv; }
+      const double dvu = vsu - vs0u, dvv = vsv - vs0v;
+      double gi1 = 0.0, cg1 = 0.0;
+      if (nrow) {
+        gi1 = 0.5 * (S(R_GX, p) * bxn + S(R_GX, p + W) * bxs);
+        cg1 = 0.5 * (S(R_CE, p) * gxn + S(R_CE, p + W) * gxs);
+      }
+      const double gi2 = 0.5 * (S(R_GY, p) * bye + S(R_GY, p + 1) * byw);
+      const double cg2 = 0.5 * (S(R_CN, p) * gye + S(R_CN, p + 1) * gyw);
+      const double sch = S(R_SCHE, p);
+      const double pg1 = (gi1 + cg1 + ghx) * seau * sch;
+      const double pg2 = (gi2 + cg2 + ghy) * seau * sch;
+      const double ubp = S(R_UB, p), vbp = S(R_VB, p);
+      double p1 = seau * (dvu + ut - pg1 + 0.5 * cor * vbp);
+      double p2 = seau * (dvv + vt - pg2 - 0.5 * cor * ubp);
+      const double w1 = p1 * bt + ubp, w2 = p2 * bt + vbp;
+      const double cb = 0.5 * cor * bt;
+      const double den = 1 + cb * cb;
+      double u1 = dvr(w1 + 0.5 * cor * bt * w2, den, rden);
+      double v1 = dvr(w2 - 0.5 * cor * bt * w1, den, rden);
+      u1 = 0.5 * (u1 + ubp);
+      v1 = 0.5 * (v1 + vbp);
+      p1 = seau * (dvu - pg1 + ut + cor * v1);
+      p2 = seau * (dvv - pg2 + vt - cor * u1);
+      const double ubc = p1 * bt + ubp, vbc = p2 * bt + vbp;
+      S(R_UBC, p) = ubc;
+      S(R_VBC, p) = vbc;
+      const double ps = prh_u * sch;
+      S(R_S1, p) = ps * ubc;
+      S(R_X2, p) = ps * vbc * rh3;
+    }
+    __syncthreads();
+    // S8: corrector ch (with the ter means of the corrector's supb), store, accumulate
+    if (inS8) {
+      const double tEc = srow ? 0.5 * (S(R_S1, p - W) + S(R_S1, p)) : 0.0;
+      const double tEw = srow ? 0.5 * (S(R_S1, p - W - 1) + S(R_S1, p - 1)) : 0.0;
+      const double A = dvr(tEc - tEw, DXX(1, lx), RDXX(1, lx));
+      double B = 0.0;
+      if (srow) {
+        const double tNc = 0.5 * (S(R_X2, p - 1) + S(R_X2, p));
+        const double tNs = 0.5 * (S(R_X2, p - W - 1) + S(R_X2, p - W));
+        B = dvr(tNc - tNs, DXY(1, ly), RDXY(1, ly));
+      }
+      const double div = dvr(A + B, vy[12 * H + ly], vy[13 * H + ly]);
+      const double chn = S(R_CH, p) - dvr(mskt1 * div * bt, prh_t, rprh_t);
+      const double ubc = S(R_UBC, p), vbc = S(R_VBC, p);
+      const int d2 = d;
+      st2(P.tr_ch[d2], P, i, q, chn);
+      st2(P.tr_ub[d2], P, i, q, ubc);
+      st2(P.tr_vb[d2], P, i, q, vbc);
+      if (nt <= nstep / 2) acc_m = acc_m + chn;
+      acc_m2 = acc_m2 + chn;
+      acc_u = acc_u + ubc;
+      acc_v = acc_v + vbc;
+    }
+    if (!grid_barrier(P, nblocks)) return;
+  }
+  if (inS8) {
+    const double ub = acc_u / (nstep + 1), vb = acc_v / (nstep + 1);
+    const double mch = acc_m / (nstep / 2 + 1), mch2 = acc_m2 / (nstep + 1);
+    st2(P.ubc, P, i, q, ub);
+    st2(P.vbc, P, i, q, vb);
+    st2(P.ubp, P, i, q, ub);
+    st2(P.vbp, P, i, q, vb);
+    st2(P.mch, P, i, q, mch);
+    st2(P.mch2, P, i, q, mch2);
+    st2(P.chc, P, i, q, mch2);
+    st2(P.chp, P, i, q, mch2);
+    st2(P.acch, P, i, q, P.acch[q] + mch2);
+  }
+}
+
+
+size_t trop_fast_smem_bytes(int TX, int TY) {
+  return ((size_t)R_COUNT * (TX + 4) * (TY + 4) + 8 * (TX + 4) + 19 * (TY + 4)) * sizeof(double);
+}
+
+cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, cudaStream_t s) {
+  const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
+  const size_t smem = trop_fast_smem_bytes(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(k_trop_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
+  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx};
+  return cudaLaunchCooperativeKernel((const void *)k_trop_fast, dim3(ntx * nty), dim3(nthreads), args, smem, s);
+}
+
+int trop_fast_max_blocks(int TX, int TY) {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = trop_fast_smem_bytes(TX, TY);
+  if (cudaFuncSetAttribute(k_trop_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_fast, nthreads, smem) != cudaSuccess) return 0;
+  return per * nsm;
+}

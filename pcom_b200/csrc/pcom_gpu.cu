@@ -10,6 +10,7 @@
 // (mod_int.f90:496-497).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -206,7 +207,7 @@ int pick_trop_config(pcom_handle *h) {
   h->trop_resident = false;
   if (h->D.separable) {
     int best_n = 1 << 30, bx = 0, by = 0;
-    const int mb = trop_res_max_blocks(24, 18);
+    const int mb = trop_fast_max_blocks(24, 18);
     for (int ty = 6; ty <= 40; ++ty)
       for (int tx = 6; tx <= 60; ++tx) {
         if (!trop_res_fits(tx, ty)) continue;
@@ -214,7 +215,7 @@ int pick_trop_config(pcom_handle *h) {
         if (nt > mb) continue;
         if (nt < best_n || (nt == best_n && (tx + 4) * (ty + 4) < (bx + 4) * (by + 4))) { best_n = nt; bx = tx; by = ty; }
       }
-    if (bx > 0 && trop_res_max_blocks(bx, by) >= best_n) {
+    if (bx > 0 && trop_fast_max_blocks(bx, by) >= best_n) {
       h->trop_resident = true;
       h->trop_tx = bx;
       h->trop_ty = by;
@@ -285,13 +286,17 @@ int do_trop(pcom_handle *h) {
     if (rc) return rc;
   }
   Prof p(h, "int_trop");
-  cudaError_t e = h->trop_resident ? launch_trop_res(h->D, h->trop_tx, h->trop_ty, h->stream)
+  cudaError_t e = h->trop_resident ? launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->stream)
                                    : launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "barotropic kernel launch: %s", cudaGetErrorString(e));
   h->n_ch++;
   return PCOM_OK;
 }
 int do_clin(pcom_handle *h) {
+  {
+    Prof p(h, "clin_2d");
+    launch_uv2d(h->D, 2, h->stream);
+  }
   {
     Prof p(h, "int_clin");
     launch_clin(h->D, h->stream);
@@ -449,10 +454,21 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   }
   double *tn3; A(&tn3, n2); D.tn3 = tn3;
   for (int g = 1; g <= 4; ++g) {
-    double *x, *y, *r;
+    double *x, *y, *r, *rx, *ry, *rr, *ar, *rar;
     A(&x, d.ni); A(&y, d.nj); A(&r, d.nj);
+    A(&rx, d.ni); A(&ry, d.nj); A(&rr, d.nj); A(&ar, d.nj); A(&rar, d.nj);
     D.dxx1d[g] = x; D.dxy1d[g] = y; D.rh1d[g] = r;
+    D.rdxx1d[g] = rx; D.rdxy1d[g] = ry; D.rrh1d[g] = rr; D.arh1d[g] = ar; D.rarh1d[g] = rar;
   }
+  {
+    double *x, *y;
+    A(&x, d.nj); A(&y, d.nj); D.aarh3 = x; D.raarh3 = y;
+    A(&x, d.nj); A(&y, d.nj); D.dys1d = x; D.rdys1d = y;
+    A(&x, n2); D.rprh_t = x; A(&x, n2); D.rprh_u = x; A(&x, n2); D.rwc = x; A(&x, n2); D.rwt = x;
+    A(&x, n2); D.dxs = x; A(&x, n2); D.rdxs = x;
+  }
+  A(&D.rsch, n2); A(&D.rsch2, n2); A(&D.rchc, n2); A(&D.rmch, n2); A(&D.rgm2, n2);
+  A(&D.schc, n2); A(&D.schu, n2); A(&D.rmch2, n2);
   int *lt = nullptr, *lu = nullptr;
   if (!rc) rc = h->alloc(&lt, (size_t)n2);
   if (!rc) rc = h->alloc(&lu, (size_t)n2);
@@ -538,27 +554,82 @@ int pcom_gpu_upload_static(pcom_handle *h, const pcom_static *s) {
     CK(cudaMemcpy((void *)D.dxx[g], bx.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void *)D.dxy[g], by.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
   }
-  // lat-lon metrics: dx?x(i, j) = dx?x(i), dx?y(i, j) = dx?y(j), rh?(i, j) = rh?(j)
+  // lat-lon metrics: dx?x(i, j) = dx?x(i), dx?y(i, j) = dx?y(j), rh?(i, j) = rh?(j),
+  // as set_hgrid builds them from 1-D lon/lat (main.f90:408-493).  Kept as
+  // 1-D vectors with the correctly rounded reciprocal of every divisor the
+  // step uses (IEEE division on the host), so kernels divide with dvr.
   {
-    bool sep = true;
-    std::vector<double> x1((size_t)ni), y1((size_t)nj), r1((size_t)nj);
-    for (int g = 1; g <= 4 && sep; ++g) {
+    const double a = D.c.a;
+    std::vector<double> x1((size_t)ni), y1((size_t)nj), r1((size_t)nj), v((size_t)std::max(ni, nj));
+    for (int g = 1; g <= 4; ++g) {
       const double *dx = s->dx[g - 1], *rh = s->rh[g - 1];
-      for (int j = 0; j < nj && sep; ++j)
+      for (int j = 0; j < nj; ++j)
         for (int i = 0; i < ni; ++i) {
           const long long q = i + (long long)ni * j;
           if (dx[2 * q] != dx[2 * (long long)i] || dx[2 * q + 1] != dx[2 * ((long long)ni * j) + 1] ||
-              rh[q] != rh[(long long)ni * j]) { sep = false; break; }
+              rh[q] != rh[(long long)ni * j])
+            return fail(PCOM_ERR_ARG, "grid %d metrics are not those of a lat-lon grid (point %d, %d)", g, i + 1, j + 1);
         }
-      if (!sep) break;
       for (int i = 0; i < ni; ++i) x1[i] = dx[2 * (long long)i];
       for (int j = 0; j < nj; ++j) { y1[j] = dx[2 * ((long long)ni * j) + 1]; r1[j] = rh[(long long)ni * j]; }
-      CK(cudaMemcpy((void *)D.dxx1d[g], x1.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy((void *)D.dxy1d[g], y1.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy((void *)D.rh1d[g], r1.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
+      auto up = [&](const double *dst, const std::vector<double> &src, int n) -> int {
+        CK(cudaMemcpy((void *)dst, src.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+        return PCOM_OK;
+      };
+      int rc = 0;
+      rc |= up(D.dxx1d[g], x1, ni);
+      rc |= up(D.dxy1d[g], y1, nj);
+      rc |= up(D.rh1d[g], r1, nj);
+      for (int i = 0; i < ni; ++i) v[i] = 1.0 / x1[i];
+      rc |= up(D.rdxx1d[g], v, ni);
+      for (int j = 0; j < nj; ++j) v[j] = 1.0 / y1[j];
+      rc |= up(D.rdxy1d[g], v, nj);
+      for (int j = 0; j < nj; ++j) v[j] = 1.0 / r1[j];
+      rc |= up(D.rrh1d[g], v, nj);
+      for (int j = 0; j < nj; ++j) v[j] = a * r1[j];
+      rc |= up(D.arh1d[g], v, nj);
+      for (int j = 0; j < nj; ++j) v[j] = 1.0 / (a * r1[j]);
+      rc |= up(D.rarh1d[g], v, nj);
+      if (g == 3) {
+        for (int j = 0; j < nj; ++j) v[j] = a * a * r1[j];
+        rc |= up(D.aarh3, v, nj);
+        for (int j = 0; j < nj; ++j) v[j] = 1.0 / (a * a * r1[j]);
+        rc |= up(D.raarh3, v, nj);
+      }
+      if (rc) return rc;
     }
-    D.separable = sep ? 1 : 0;
+    D.separable = 1;
     h->trop_blocks = 0;  // re-pick the barotropic kernel configuration
+    // smag's dy (j) and dx (i, j) (mod_int.f90:416-418) and their reciprocals
+    const double *dx2 = s->dx[1], *dx4 = s->dx[3], *rh4 = s->rh[3];
+    for (int j = 0; j < nj; ++j) v[j] = (j + 1 < nj) ? a * (dx2[2 * ((long long)ni * j) + 1] + dx2[2 * ((long long)ni * (j + 1)) + 1]) : 1.0;
+    CK(cudaMemcpy((void *)D.dys1d, v.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
+    for (int j = 0; j < nj; ++j) v[j] = 1.0 / v[j];
+    CK(cudaMemcpy((void *)D.rdys1d, v.data(), nj * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> w2((size_t)n2, 1.0), rw2((size_t)n2, 1.0);
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i + 1 < ni; ++i) {
+        const long long q = i + (long long)ni * j;
+        w2[q] = a * (rh4[q] * dx4[2 * q] + rh4[q + 1] * dx4[2 * (q + 1)]);
+        rw2[q] = 1.0 / w2[q];
+      }
+    CK(cudaMemcpy((void *)D.dxs, w2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void *)D.rdxs, rw2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    // 1/prh, and the Coriolis-adjustment denominators 1 + (0.5 cor dt)^2
+    // (mod_int.f90:246, 358-361) for dtbt and dtbc
+    for (long long q = 0; q < n2; ++q) { w2[q] = 1.0 / s->prh_t[q]; rw2[q] = 1.0 / s->prh_u[q]; }
+    CK(cudaMemcpy((void *)D.rprh_t, w2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void *)D.rprh_u, rw2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    for (long long q = 0; q < n2; ++q) {
+      const double wc = 0.5 * s->cor[q] * (double)D.bc, wt = 0.5 * s->cor[q] * (double)D.bt;
+      w2[q] = 1.0 / (1 + wc * wc);
+      rw2[q] = 1.0 / (1 + wt * wt);
+    }
+    CK(cudaMemcpy((void *)D.rwc, w2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void *)D.rwt, rw2.data(), n2 * sizeof(double), cudaMemcpyHostToDevice));
+    D.ra = 1.0 / a;
+    D.rg = 1.0 / D.c.g;
+    D.rbc32 = 1.0 / (double)(4 * 8 * D.bc);
   }
   if (!s->tn[2]) return fail(PCOM_ERR_ARG, "tn of grid 3 missing");
   CK(cudaMemcpy((void *)D.tn3, s->tn[2], n2 * sizeof(double), cudaMemcpyHostToDevice));
@@ -574,8 +645,8 @@ int pcom_gpu_upload_static(pcom_handle *h, const pcom_static *s) {
   CK(cudaMemcpy((void *)D.km, s->km, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy((void *)D.kh, s->kh, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
   if (!s->pr2 || !s->dpr2 || !s->dz1) return fail(PCOM_ERR_ARG, "vertical grid missing");
-  for (int k = 1; k <= nk; ++k) { D.pr2[k] = s->pr2[k - 1]; D.dpr2[k] = s->dpr2[k - 1]; }
-  for (int k = 1; k <= nkp; ++k) D.dz1[k] = s->dz1[k - 1];
+  for (int k = 1; k <= nk; ++k) { D.pr2[k] = s->pr2[k - 1]; D.dpr2[k] = s->dpr2[k - 1]; D.rdpr2[k] = 1.0 / s->dpr2[k - 1]; }
+  for (int k = 1; k <= nkp; ++k) { D.dz1[k] = s->dz1[k - 1]; D.rdz1[k] = 1.0 / s->dz1[k - 1]; }
   (void)ni; (void)nj;
   h->static_ok = true;
   return PCOM_OK;

@@ -22,6 +22,10 @@ size_t trop_res_smem_bytes(int TX, int TY);
 bool trop_res_fits(int TX, int TY);
 cudaError_t launch_trop_res(const Dev &P, int TX, int TY, cudaStream_t s);
 int trop_res_max_blocks(int TX, int TY);
+// the same with reciprocal divisions (handle path)
+size_t trop_fast_smem_bytes(int TX, int TY);
+cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, cudaStream_t s);
+int trop_fast_max_blocks(int TX, int TY);
 
 // the model constants (literal precision per PCOM_LIT_R8)
 void pcom_dev_consts(bool r8, DevConsts &c);
