@@ -674,7 +674,7 @@ int trop_res_max_blocks(int TX, int TY) {
 // reciprocal-approximation instruction from the critical path.
 
 __global__ void __launch_bounds__(kResThreads, 1)
-    k_trop_fast(const __grid_constant__ Dev P, int TX, int TY, int ntx) {
+    k_trop_fast(const __grid_constant__ Dev P, int TX, int TY, int ntx, unsigned long long epoch) {
   extern __shared__ double sm[];
   const int ni = P.ni, nj = P.nj, njm = P.njm, G = P.glo_ni;
   const int W = TX + 4, H = TY + 4, RS = W * H;
@@ -682,7 +682,6 @@ __global__ void __launch_bounds__(kResThreads, 1)
   double *vy = vx + 8 * W;         // kFastVy vectors over ly (see below)
   const double a = P.c.a, bt = (double)P.bt, gamma_b = P.c.gamma_b;
   const int nstep = P.nstep;
-  const unsigned nblocks = gridDim.x;
   const int tid = threadIdx.x;
   const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
   const int R0 = tx * TX, J0 = ty * TY + 1;
@@ -762,15 +761,16 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const double land_ch0 = inS4 ? P.chc[q] : 0.0;
   __syncthreads();
 
+  const unsigned long long base = epoch;  // arrivals counted before this launch
   for (int nt = 1; nt <= nstep; ++nt) {
     const int d = (nt - 1) & 1;
     const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
     const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
     const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
     // S1: previous state
-    if (active) {
-      S(R_CH, p) = src_ch[q];
-      if (inS2) { S(R_UB, p) = src_ub[q]; S(R_VB, p) = src_vb[q]; }
+    if (active) {  // L2 loads (.cg): the buffers were written by other SMs
+      S(R_CH, p) = __ldcg(src_ch + q);
+      if (inS2) { S(R_UB, p) = __ldcg(src_ub + q); S(R_VB, p) = __ldcg(src_vb + q); }
     }
     __syncthreads();
     // S2: sch = sqrt(ter(ch)) on U, supb
@@ -906,7 +906,27 @@ __global__ void __launch_bounds__(kResThreads, 1)
       acc_u = acc_u + ubc;
       acc_v = acc_v + vbc;
     }
-    if (!grid_barrier(P, nblocks)) return;
+    // grid barrier on a monotone arrival counter: each CTA adds 1 after
+    // making its writes visible, then waits (bounded) for all arrivals of
+    // this substep; the counter is never reset, targets grow per launch
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(P.tile_flag, 1ULL);
+      const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*P.tile_flag);
+      cuda::atomic_ref<int, cuda::thread_scope_device> err(P.err[0]);
+      long long it = 0;
+      while (c.load(cuda::memory_order_acquire) < want) {
+        if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
+          err.store(1, cuda::memory_order_relaxed);
+          break;
+        }
+        if (it > 1024) __nanosleep(32);
+      }
+    }
+    __syncthreads();
+    if (*(volatile int *)P.err != 0) return;
   }
   if (inS8) {
     const double ub = acc_u / (nstep + 1), vb = acc_v / (nstep + 1);
@@ -928,13 +948,13 @@ size_t trop_fast_smem_bytes(int TX, int TY) {
   return ((size_t)R_COUNT * (TX + 4) * (TY + 4) + 8 * (TX + 4) + 19 * (TY + 4)) * sizeof(double);
 }
 
-cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, cudaStream_t s) {
+cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
   const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
   const size_t smem = trop_fast_smem_bytes(TX, TY);
   cudaError_t e = cudaFuncSetAttribute(k_trop_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
-  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx};
+  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch};
   return cudaLaunchCooperativeKernel((const void *)k_trop_fast, dim3(ntx * nty), dim3(nthreads), args, smem, s);
 }
 

@@ -63,6 +63,7 @@ struct Dev {
   double *tr_ch[2], *tr_ub[2], *tr_vb[2];
   double *tr_acc[6];  // mch, mch2, ub, vb accumulators; first-substep viscosity (u, v)
   unsigned *bar;   // [0] arrival count, [1] generation
+  unsigned long long *tile_flag;  // per-tile progress of the barotropic kernel (monotone across launches)
   int *err;        // [0] timeout flag, [1] watchdog flag
   // lat-lon (separable) metrics: dx?x depends on i only, dx?y and rh? on j
   // only (set_hgrid builds them from 1-D lon/lat, main.f90:408-493); when the

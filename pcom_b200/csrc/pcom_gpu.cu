@@ -134,6 +134,7 @@ struct pcom_handle {
   int n_ts = 0, n_uv = 0, n_w = 0, n_ch = 0, n_ssh = 0;
   int trop_tx = 24, trop_ty = 18, trop_blocks = 0;
   bool trop_resident = false;
+  unsigned long long trop_epoch = 0;  // barrier arrivals of the barotropic kernel so far
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
   long long launches = 0;
@@ -184,6 +185,8 @@ int sync_check(pcom_handle *h) {
   if (err[0]) {
     cudaMemset(h->D.err, 0, sizeof err);
     cudaMemset(h->D.bar, 0, 2 * sizeof(unsigned));
+    cudaMemset(h->D.tile_flag, 0, sizeof(unsigned long long));
+    h->trop_epoch = 0;
     return fail(PCOM_ERR_TIMEOUT, "a device-side grid barrier gave up waiting (bounded spin)");
   }
   return PCOM_OK;
@@ -286,8 +289,14 @@ int do_trop(pcom_handle *h) {
     if (rc) return rc;
   }
   Prof p(h, "int_trop");
-  cudaError_t e = h->trop_resident ? launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->stream)
-                                   : launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
+  cudaError_t e;
+  if (h->trop_resident) {
+    // the kernel's barrier counter is monotone: pass the arrivals so far
+    e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
+    h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
+  } else {
+    e = launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
+  }
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "barotropic kernel launch: %s", cudaGetErrorString(e));
   h->n_ch++;
   return PCOM_OK;
@@ -501,6 +510,11 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   if (!rc) rc = h->alloc(&bar, 4);
   if (!rc) rc = h->alloc(&err, 4);
   if (!rc) rc = h->alloc(&h->d_count, 1);
+  {
+    unsigned long long *tf = nullptr;
+    if (!rc) rc = h->alloc(&tf, 4096);
+    D.tile_flag = tf;
+  }
   D.bar = bar; D.err = err;
   if (rc) { pcom_gpu_destroy(h); return rc; }
   // reference initial values (mod_arrays.f90:298-313): alpha = 1/1000.0, am = am_c, ch = 1

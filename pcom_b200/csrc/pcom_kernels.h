@@ -24,7 +24,7 @@ cudaError_t launch_trop_res(const Dev &P, int TX, int TY, cudaStream_t s);
 int trop_res_max_blocks(int TX, int TY);
 // the same with reciprocal divisions (handle path)
 size_t trop_fast_smem_bytes(int TX, int TY);
-cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, cudaStream_t s);
+cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
 int trop_fast_max_blocks(int TX, int TY);
 
 // the model constants (literal precision per PCOM_LIT_R8)
