@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P)
 // ----------------------------------------------------------------------------
 // int_clin (mod_int.f90:298-396): baroclinic momentum, barotropic
 // replacement, unweighted velocity and its accumulation.  smag runs after.
-__global__ void __launch_bounds__(512) k_clin(const __grid_constant__ Dev P) {
+__global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P) {
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *t1s = sh, *t2s = sh + nk * TB_X, *wsum = sh + 2 * nk * TB_X;
@@ -580,10 +580,12 @@ __global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ Dev P) {
 // (mod_op.f90:280-325), diffusion op_dif (mod_op.f90:186-222), surface
 // restoring, time step, ice floor, convective adjustment (convect/adjust/mix,
 // mod_int.f90:509-600), tp = tc, and the act/acs/acr accumulations.
-struct Col {  // one column of T and S in shared memory, stride TB_X
-  double *t, *s;
+struct Col {  // one column of T, S and prho in shared memory, stride TB_X
+  double *t, *s, *p1, *p2;
   __device__ double &T(int k) { return t[(k - 1) * TB_X]; }
   __device__ double &S(int k) { return s[(k - 1) * TB_X]; }
+  __device__ double P1(int k) const { return p1[(k - 1) * TB_X]; }
+  __device__ double P2(int k) const { return p2[(k - 1) * TB_X]; }
 };
 
 __device__ void ts_mix(const Dev &P, long long q2, Col &c, double *rhoa, double *rhob, int na, int nb) {
@@ -596,31 +598,16 @@ __device__ void ts_mix(const Dev &P, long long q2, Col &c, double *rhoa, double 
   for (int k = na; k <= nb; ++k) ss = ss + c.S(k) * P.dpr2[k];
   const double sn = ss / sd;
   for (int k = na; k <= nb; ++k) c.S(k) = sn;
-  for (int k = na; k <= nb; ++k) {
-    const double2 pr = P.prho[q2 + P.n2 * (k - 1)];
-    rhoa[k] = pr.x * c.T(k) + pr.y * c.S(k);
-  }
-  for (int k = na; k <= nb - 1; ++k) {
-    const double2 pr = P.prho[q2 + P.n2 * k];
-    rhob[k] = pr.x * c.T(k) + pr.y * c.S(k);
-  }
-  if (nb < P.nk) {
-    const double2 pr = P.prho[q2 + P.n2 * nb];
-    rhob[nb] = pr.x * c.T(nb) + pr.y * c.S(nb);
-  }
+  for (int k = na; k <= nb; ++k) rhoa[k] = c.P1(k) * c.T(k) + c.P2(k) * c.S(k);
+  for (int k = na; k <= nb - 1; ++k) rhob[k] = c.P1(k + 1) * c.T(k) + c.P2(k + 1) * c.S(k);
+  if (nb < P.nk) rhob[nb] = c.P1(nb + 1) * c.T(nb) + c.P2(nb + 1) * c.S(nb);
 }
 
 __device__ void ts_convect(const Dev &P, long long q2, int nlev, Col c) {
   double rhoa[PCOM_MAXK + 2], rhob[PCOM_MAXK + 2];
   for (int k = 0; k <= P.nk + 1; ++k) { rhoa[k] = 0.0; rhob[k] = 0.0; }
-  for (int k = 2; k <= nlev; ++k) {
-    const double2 pr = P.prho[q2 + P.n2 * (k - 1)];
-    rhoa[k] = pr.x * c.T(k) + pr.y * c.S(k);
-  }
-  for (int k = 1; k <= nlev - 1; ++k) {
-    const double2 pr = P.prho[q2 + P.n2 * k];
-    rhob[k] = pr.x * c.T(k) + pr.y * c.S(k);
-  }
+  for (int k = 2; k <= nlev; ++k) rhoa[k] = c.P1(k) * c.T(k) + c.P2(k) * c.S(k);
+  for (int k = 1; k <= nlev - 1; ++k) rhob[k] = c.P1(k + 1) * c.T(k) + c.P2(k + 1) * c.S(k);
   int kcnt = 1, guard = 0;
   while (kcnt < nlev && guard < 4 * PCOM_MAXK * PCOM_MAXK) {
     ++guard;
@@ -653,13 +640,15 @@ __device__ void ts_convect(const Dev &P, long long q2, int nlev, Col c) {
 __global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P) {
   extern __shared__ double sh[];
   const int nk = P.nk;
-  double *tcs = sh, *scs = sh + nk * TB_X;
+  double *tcs = sh, *scs = sh + nk * TB_X, *p1s = sh + 2 * nk * TB_X, *p2s = sh + 3 * nk * TB_X;
+  __shared__ int unstable[TB_X];
   int i, j;
   const bool ok = cell(P, i, j, true);
   const int tx = threadIdx.x;
   const long long q2 = ok ? I2(P, i, j) : 0;
   const int ni = P.ni;
   const double g = P.c.g;
+  if (threadIdx.y == 0) unstable[tx] = 0;
   const double grho = g * P.c.rho0;
   const bool nrow = j <= P.njm, srow = j >= 2;
   const long long qw = q2 - 1, qs = q2 - ni, qsw = qs - 1, qe = q2 + 1, qn = q2 + ni;
@@ -752,10 +741,22 @@ __global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P) {
     if (m_c > 0 && tn < P.c.tice) tn = P.c.tice;
     tcs[(k - 1) * TB_X + tx] = tn;
     scs[(k - 1) * TB_X + tx] = sn;
+    const double2 pr = P.prho[q];
+    p1s[(k - 1) * TB_X + tx] = pr.x;
+    p2s[(k - 1) * TB_X + tx] = pr.y;
   }
   __syncthreads();
-  if (ok && threadIdx.y == 0 && lev > 1) {
-    Col c{tcs + tx, scs + tx};
+  // the adjustment scan of convect starts only where rhob(k) > rhoa(k+1)
+  // for some 1 <= k < nlev (mod_int.f90:530-537); test every level at once
+  for (int k = threadIdx.y + 1; k < lev && ok; k += TB_K) {
+    const int o = (k - 1) * TB_X + tx, o1 = k * TB_X + tx;
+    const double rb = p1s[o1] * tcs[o] + p2s[o1] * scs[o];
+    const double ra = p1s[o1] * tcs[o1] + p2s[o1] * scs[o1];
+    if (rb > ra) unstable[tx] = 1;
+  }
+  __syncthreads();
+  if (ok && threadIdx.y == 0 && lev > 1 && unstable[tx]) {
+    Col c{tcs + tx, scs + tx, p1s + tx, p2s + tx};
     ts_convect(P, q2, lev, c);
   }
   __syncthreads();
@@ -824,5 +825,5 @@ void launch_smag(const Dev &P, cudaStream_t s) {
   if (P.nj > 2) k_smag<<<g, dim3(32, 4), 0, s>>>(P);
 }
 void launch_ssh(const Dev &P, cudaStream_t s) { k_ssh<<<grid3(P, false), kBlock3, sm3(P, 1), s>>>(P); }
-void launch_ts(const Dev &P, cudaStream_t s) { k_ts<<<grid3(P, true), kBlock3, sm3(P, 2), s>>>(P); }
+void launch_ts(const Dev &P, cudaStream_t s) { k_ts<<<grid3(P, true), kBlock3, sm3(P, 4), s>>>(P); }
 void launch_den_prho(const Dev &P, cudaStream_t s) { k_den_prho<<<grid3(P, false), kBlock3, 0, s>>>(P); }
