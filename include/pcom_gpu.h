@@ -160,6 +160,35 @@ int pcom_gpu_profile_read(pcom_handle *h, char *names, int64_t *launches, double
 /* Number of this library's kernel launches issued so far on this handle. */
 int64_t pcom_gpu_launch_count(pcom_handle *h);
 
+/* --- batches -------------------------------------------------------------- */
+/* No counterpart in the reference (it runs one domain per MPI job).  A batch
+ * steps several handles together -- ensemble members and basins of uneven
+ * size that share dtbt and dtbc -- with every kernel of the step launched
+ * once for all members and the barotropic subcycles of all members in one
+ * persistent cooperative launch over the work list of their tiles.  After the
+ * two AB3 start-up steps the whole batched step is replayed from a captured
+ * CUDA graph.  Members must be advanced only through the batch (their ring
+ * buffers rotate in lock step); each member's handle still serves its state,
+ * fields and accumulators. */
+typedef struct pcom_batch pcom_batch;
+int pcom_gpu_batch_create(pcom_handle *const *members, int32_t n, pcom_batch **out);
+int pcom_gpu_batch_destroy(pcom_batch *b);
+/* One baroclinic step of every member (main.f90:205-223), tctr_i as in pcom_gpu_step. */
+int pcom_gpu_batch_step(pcom_batch *b, int64_t tctr_i);
+int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i);
+/* Wait for the batch's enqueued work (on the first member's stream) and
+ * report a barrier timeout; call it before reading a member after
+ * pcom_gpu_batch_step_async. */
+int pcom_gpu_batch_sync(pcom_batch *b);
+/* den_prho of every member (mod_den.f90:120-153). */
+int pcom_gpu_batch_den_prho(pcom_batch *b);
+/* Replay captured CUDA graphs (default on) or launch kernel by kernel. */
+int pcom_gpu_batch_use_graphs(pcom_batch *b, int32_t enable);
+/* Time candidate tile shapes of the batched barotropic kernel on the
+ * members' current state (which it saves and restores) and keep the fastest;
+ * a one-line report of the trials goes to `report`. */
+int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len);
+
 /* --- allocation-free barotropic subcycle -------------------------------- */
 /* No counterpart in the reference.  One int_trop subcycle (the same kernel
  * and arithmetic as pcom_gpu_step uses) over arrays the caller owns, for

@@ -47,6 +47,12 @@ int pcom_model_destroy(pcom_model *m);
 pcom_handle *pcom_model_handle(pcom_model *m);
 /* n passes of the time loop body (main.f90:158-238, without output()). */
 int pcom_model_run(pcom_model *m, int64_t nsteps);
+/* n passes of the time loop for n models stepped together through batch b
+ * (pcom_gpu_batch_create on their handles, in the same order).  The models
+ * must be at the same iteration and date (same bdate and dtbc): forcing
+ * (int_bnd) is interpolated per model on day changes, then den_prho and the
+ * step run batched.  No counterpart in the reference. */
+int pcom_model_run_batch(pcom_model *const *ms, int32_t n, pcom_batch *b, int64_t nsteps);
 /* tctr%i of the last completed step, and the model date tctr%ct. */
 int64_t pcom_model_iter(pcom_model *m);
 int pcom_model_date(pcom_model *m, int32_t *ymdh4);

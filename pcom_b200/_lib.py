@@ -101,10 +101,19 @@ SIGNATURES = {
     "pcom_gpu_launch_count": (C.c_int64, [C.c_void_p]),
     "pcom_gpu_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
     "pcom_gpu_trop_noalloc": (C.c_int, [C.POINTER(TropIO), C.c_void_p]),
+    "pcom_gpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+    "pcom_gpu_batch_destroy": (C.c_int, [C.c_void_p]),
+    "pcom_gpu_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),
+    "pcom_gpu_batch_step_async": (C.c_int, [C.c_void_p, C.c_int64]),
+    "pcom_gpu_batch_den_prho": (C.c_int, [C.c_void_p]),
+    "pcom_gpu_batch_sync": (C.c_int, [C.c_void_p]),
+    "pcom_gpu_batch_use_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcom_gpu_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "pcom_model_create": (C.c_int, [C.POINTER(Case), C.c_int32, C.POINTER(C.c_void_p)]),
     "pcom_model_destroy": (C.c_int, [C.c_void_p]),
     "pcom_model_handle": (C.c_void_p, [C.c_void_p]),
     "pcom_model_run": (C.c_int, [C.c_void_p, C.c_int64]),
+    "pcom_model_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_void_p, C.c_int64]),
     "pcom_model_iter": (C.c_int64, [C.c_void_p]),
     "pcom_model_date": (C.c_int, [C.c_void_p, i32_p]),
     "pcom_model_static": (C.c_int, [C.c_void_p, C.POINTER(Static)]),

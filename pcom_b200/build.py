@@ -17,7 +17,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpcomgpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_FP64 = ["k_step.cu", "k_trop.cu", "pcom_gpu.cu", "k_trop_noalloc.cu"]
+CU_FP64 = ["k_step.cu", "k_trop.cu", "pcom_gpu.cu", "k_trop_noalloc.cu", "k_trop_batch.cu"]
 CU_FAST = []  # kernels allowed to contract a*b+c into FMA (mixed precision)
 CPP = ["pcom_host.cpp"]
 

@@ -44,16 +44,18 @@ __device__ __forceinline__ bool cell(const Dev &P, int &i, int &j, bool interior
   j = blockIdx.y + 1;
   if (interior) {
     i = x + 2;
-    return x < P.glo_ni;
+    return x < P.glo_ni && j <= P.nj;
   }
   i = x + 1;
-  return i <= P.ni;
+  return i <= P.ni && j <= P.nj;
 }
 
 // ----------------------------------------------------------------------------
 // den_alpha (mod_den.f90:33-55) with T, S = tc, sc and ch = chc, fused with
 // int_tobot (mod_op.f90:927-944) -> adp.
-__global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   double *tmp = sh;  // [nk][TB_X]
   int i, j;
@@ -94,7 +96,9 @@ __global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev
 // int_pgra (mod_int.f90:64-88): bphi and bgraphi, the column integrals of the
 // E/N-averaged geopotential and of the adp gradient (op_vint_ns/op_vint_ew,
 // mod_op.f90:946-981, incl. their cshift(-1) masks).
-__global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *bE = sh, *bN = sh + nk * TB_X, *bX = sh + 2 * nk * TB_X, *bY = sh + 3 * nk * TB_X;
@@ -149,7 +153,9 @@ __global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P) {
 //     1/mch, 1/(g mch2)
 //  mode 2 (int_clin, mod_int.f90:318-320, 385-386): sqrt(ter(mch, dft 1))
 //     with 1 on land, sqrt(ter(mch2, dft 1)), 1/mch2
-__global__ void k_uv2d(const __grid_constant__ Dev P, int mode) {
+template <bool BATCH>
+__global__ void k_uv2d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, int mode) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   if (x >= P.glo_ni || j > P.nj) return;
@@ -192,7 +198,9 @@ __global__ void k_uv2d(const __grid_constant__ Dev P, int mode) {
 // upwelling (mod_int.f90:626-647): wk3d = div(sqrt(ter(chp)) * (uc, vc)),
 // wm(k) = (wm(k-1) + dpr(k-1) (wk3d(k-1) - vint(wk3d))) msk(k).
 // with_acw: also int_ts's acw accumulation (mod_int.f90:458-461).
-__global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P, int with_acw) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, int with_acw) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *wk = sh, *tm = sh + nk * TB_X, *wmv = sh + 2 * nk * TB_X;
@@ -255,7 +263,9 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P
 // int_readyc 3-D part (mod_int.f90:114-149): op_adv for uc and vc
 // (mod_op.f90:224-278), op_fri -> fri_r3d for both components
 // (mod_op.f90:103-184) and the depth integral of the baroclinic tendency.
-__global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *tu = sh, *tv = sh + nk * TB_X;
@@ -415,7 +425,9 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P)
 // ----------------------------------------------------------------------------
 // int_clin (mod_int.f90:298-396): baroclinic momentum, barotropic
 // replacement, unweighted velocity and its accumulation.  smag runs after.
-__global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *t1s = sh, *t2s = sh + nk * TB_X, *wsum = sh + 2 * nk * TB_X;
@@ -521,18 +533,21 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P) 
 
 // ----------------------------------------------------------------------------
 // smag (mod_int.f90:403-440): Smagorinsky viscosity, rows 2..nj-1.
-__global__ void k_smag(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void k_smag(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int k = blockIdx.z + 1;
   if (x >= P.glo_ni || j > P.nj - 1) return;
   const int i = x + 2;
-  const long long q2 = I2(P, i, j), q = q2 + P.n2 * (k - 1);
+  const long long q2 = I2(P, i, j);
   const int ni = P.ni;
   const double dx = ld(P.dxs, q2), rdx = ld(P.rdxs, q2);
   const double dy = __ldg(P.dys1d + j - 1), rdy = __ldg(P.rdys1d + j - 1);
   const double tn = ld(P.tn3, q2);
   const double *u = P.uu, *v = P.vv;
+  for (int k = 1; k <= P.nk; ++k) {
+  const long long q = q2 + P.n2 * (k - 1);
   const double dt = dvr(4 * (ld(u, q + 1) - ld(u, q - 1)), dx, rdx) - dvr(4 * (ld(v, q + ni) - ld(v, q - ni)), dy, rdy) +
                     DIVA(ld(v, q) * tn);
   const double ds = dvr(4 * (ld(v, q + 1) - ld(v, q - 1)), dx, rdx) + dvr(4 * (ld(u, q + ni) - ld(u, q - ni)), dy, rdy) -
@@ -542,11 +557,14 @@ __global__ void k_smag(const __grid_constant__ Dev P) {
   const double wk = c * sqrt(dt * dt + ds * ds);
   const double am_max = dvr(dx * dx + dy * dy, (double)(4 * 8 * P.bc), P.rbc32);
   st2(P.am, P, i, q, wk < am_max ? wk : am_max);
+  }
 }
 
 // ----------------------------------------------------------------------------
 // int_ssh (mod_int.f90:602-624): alpha from (tp, sp, mch), SSH accumulation.
-__global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   int i, j;
@@ -637,7 +655,9 @@ __device__ void ts_convect(const Dev &P, long long q2, int nlev, Col c) {
   }
 }
 
-__global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *tcs = sh, *scs = sh + nk * TB_X, *p1s = sh + 2 * nk * TB_X, *p2s = sh + 3 * nk * TB_X;
@@ -778,7 +798,9 @@ __global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P) {
 
 // ----------------------------------------------------------------------------
 // den_prho (mod_den.f90:120-153)
-__global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ Dev P) {
+template <bool BATCH>
+__global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
+  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
   int i, j;
   if (!cell(P, i, j, false)) return;
   const long long q2 = I2(P, i, j);
@@ -801,29 +823,46 @@ __global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ Dev P)
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-static inline dim3 grid3(const Dev &P, bool interior) {
-  const int nx = interior ? P.glo_ni : P.ni;
-  return dim3((nx + TB_X - 1) / TB_X, P.nj, 1);
-}
+// Single domain: the Dev travels as a kernel parameter.  Batch: Ps[m] in
+// device memory describes member m = blockIdx.z; the grid is sized to the
+// largest member and CTAs outside a smaller member's domain do nothing.
 static const dim3 kBlock3(TB_X, TB_K, 1);
-static inline size_t sm3(const Dev &P, int planes) { return (size_t)planes * P.nk * TB_X * sizeof(double); }
+static inline dim3 g3(int nx, int ny, int nz) { return dim3((nx + TB_X - 1) / TB_X, ny, nz); }
+static inline size_t sm3(int nk, int planes) { return (size_t)planes * nk * TB_X * sizeof(double); }
 
-void launch_alpha_tobot(const Dev &P, cudaStream_t s) { k_alpha_tobot<<<grid3(P, false), kBlock3, sm3(P, 1), s>>>(P); }
-void launch_pgra2d(const Dev &P, cudaStream_t s) { k_pgra2d<<<grid3(P, true), kBlock3, sm3(P, 4), s>>>(P); }
+void launch_alpha_tobot(const Dev &P, cudaStream_t s) { k_alpha_tobot<false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+void launch_pgra2d(const Dev &P, cudaStream_t s) { k_pgra2d<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
 void launch_uv2d(const Dev &P, int mode, cudaStream_t s) {
-  k_uv2d<<<dim3((P.glo_ni + 31) / 32, (P.nj + 3) / 4), dim3(32, 4), 0, s>>>(P, mode);
+  k_uv2d<false><<<dim3((P.glo_ni + 31) / 32, (P.nj + 3) / 4), dim3(32, 4), 0, s>>>(P, nullptr, mode);
 }
 void launch_upwelling(const Dev &P, int with_acw, cudaStream_t s) {
-  k_upwelling<<<grid3(P, true), kBlock3, sm3(P, 3), s>>>(P, with_acw);
+  k_upwelling<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 3), s>>>(P, nullptr, with_acw);
 }
-void launch_readyc3d(const Dev &P, cudaStream_t s) { k_readyc3d<<<grid3(P, true), kBlock3, sm3(P, 2), s>>>(P); }
+void launch_readyc3d(const Dev &P, cudaStream_t s) { k_readyc3d<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr); }
 void launch_clin(const Dev &P, cudaStream_t s) {
-  k_clin<<<grid3(P, true), kBlock3, sm3(P, 2) + 2 * TB_X * sizeof(double), s>>>(P);
+  k_clin<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2) + 2 * TB_X * sizeof(double), s>>>(P, nullptr);
 }
 void launch_smag(const Dev &P, cudaStream_t s) {
-  dim3 g((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, P.nk);
-  if (P.nj > 2) k_smag<<<g, dim3(32, 4), 0, s>>>(P);
+  if (P.nj > 2) k_smag<false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, 1), dim3(32, 4), 0, s>>>(P, nullptr);
 }
-void launch_ssh(const Dev &P, cudaStream_t s) { k_ssh<<<grid3(P, false), kBlock3, sm3(P, 1), s>>>(P); }
-void launch_ts(const Dev &P, cudaStream_t s) { k_ts<<<grid3(P, true), kBlock3, sm3(P, 4), s>>>(P); }
-void launch_den_prho(const Dev &P, cudaStream_t s) { k_den_prho<<<grid3(P, false), kBlock3, 0, s>>>(P); }
+void launch_ssh(const Dev &P, cudaStream_t s) { k_ssh<false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+void launch_ts(const Dev &P, cudaStream_t s) { k_ts<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
+void launch_den_prho(const Dev &P, cudaStream_t s) { k_den_prho<false><<<g3(P.ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr); }
+
+void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cudaStream_t s) {
+  Dev none{};  // the by-value parameter is unused in the batched form
+  const int n = b.n;
+  switch (kernel) {
+  case BK_ALPHA_TOBOT: k_alpha_tobot<true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
+  case BK_PGRA2D: k_pgra2d<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
+  case BK_UV2D: k_uv2d<true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs, arg); break;
+  case BK_UPWELLING: k_upwelling<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 3), s>>>(none, dPs, arg); break;
+  case BK_READYC3D: k_readyc3d<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2), s>>>(none, dPs); break;
+  case BK_CLIN: k_clin<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
+  case BK_SMAG: k_smag<true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
+  case BK_SSH: k_ssh<true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
+  case BK_TS: k_ts<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
+  case BK_DEN_PRHO: k_den_prho<true><<<g3(b.ni, b.nj, n), kBlock3, 0, s>>>(none, dPs); break;
+  default: break;
+  }
+}

@@ -1,0 +1,312 @@
+// k_trop_batch.cu -- the barotropic subcycle of int_trop (mod_int.f90:153-296)
+// for a batch of domains (ensemble members and basins of uneven size) in ONE
+// persistent cooperative launch.
+//
+// The tiles of every member form one work list; each CTA owns tiles of any
+// member (possibly several) and, per substep, stages each tile's
+// (TX+4) x (TY+4) region in shared memory and evaluates the same predictor /
+// viscosity / pressure-gradient / Coriolis / corrector sequence as the
+// single-domain kernel (same operation order, divisions by reciprocals), then
+// all CTAs meet at one grid barrier.  Static coefficients are read per point
+// from the member's arrays (L2-resident); accumulators and the first
+// substep's viscosity live in the member's 2-D scratch.  All members share
+// dtbt and dtbc, so they take the same number of substeps.
+#include <cuda/atomic>
+
+#include "pcom_dev.cuh"
+#include "pcom_kernels.h"
+
+namespace {
+
+constexpr long long kSpin = 1LL << 26;
+
+enum {
+  B_CH, B_UB, B_VB, B_S1, B_X2, B_PRED, B_SCHE,
+  B_A1U, B_A1V, B_GY, B_CN, B_A2U, B_A2V, B_GX, B_CE,
+  B_UBC, B_VBC,
+  B_COUNT
+};
+
+__device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, int *err) {
+  __syncthreads();
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(cnt, 1ULL);
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*cnt);
+    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    long long it = 0;
+    int f = 0;
+    while (c.load(cuda::memory_order_acquire) < want) {
+      if (++it > kSpin || e.load(cuda::memory_order_relaxed) != 0) {
+        e.store(1, cuda::memory_order_relaxed);
+        f = 1;
+        break;
+      }
+      if (it > 1024) __nanosleep(32);
+    }
+    s_fail = f;
+  }
+  __syncthreads();
+  return s_fail == 0;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, const TileRef *__restrict__ tiles,
+                                                    int ntiles, int TX, int TY, unsigned long long *cnt, int *err) {
+  extern __shared__ double sm[];
+  const int W = TX + 4, RS = W * (TY + 4);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int nstep = Ps[0].nstep;
+  auto S = [&](int f, int p) -> double & { return sm[f * RS + p]; };
+
+  // accumulators of owned points (mod_int.f90:176-180)
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileRef T = tiles[t];
+    const Dev &P = Ps[T.m];
+    for (int p = tid; p < T.tw * T.th; p += nth) {
+      const int i = T.r0 + p % T.tw + 2, j = T.j0 + p / T.tw;
+      const long long q = I2(P, i, j);
+      P.tr_acc[0][q] = P.chc[q];
+      P.tr_acc[1][q] = P.chc[q];
+      P.tr_acc[2][q] = P.ubc[q];
+      P.tr_acc[3][q] = P.vbc[q];
+    }
+  }
+
+  for (int nt = 1; nt <= nstep; ++nt) {
+    const int d = (nt - 1) & 1;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const TileRef T = tiles[t];
+      const Dev &P = Ps[T.m];
+      const int G = P.glo_ni, nj = P.nj, njm = P.njm, ni = P.ni;
+      const int tw = T.tw, th = T.th, rr0 = T.r0 - 2, jj0 = T.j0 - 2;
+      const double a = P.c.a, ra = P.ra, bt = (double)P.bt, gamma_b = P.c.gamma_b;
+      const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
+      const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
+      const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
+      auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
+      // region point p -> (lx, ly, i, j, q); valid rows only
+#define PT(nx, lo_x, lo_y)                                  \
+  const int lx = (lo_x) + pp % (nx), ly = (lo_y) + pp / (nx); \
+  const int j = jj0 + ly;                                   \
+  if (j < 1 || j > nj) continue;                            \
+  const int i = ring_i(rr0 + lx);                           \
+  const long long q = I2(P, i, j);                          \
+  const int p = ly * W + lx;                                \
+  (void)i;
+      // S1: previous state (L2 loads: written by other CTAs)
+      for (int pp = tid; pp < (tw + 4) * (th + 4); pp += nth) {
+        PT(tw + 4, 0, 0)
+        S(B_CH, p) = __ldcg(src_ch + q);
+        if (lx < tw + 3 && ly < th + 3) { S(B_UB, p) = __ldcg(src_ub + q); S(B_VB, p) = __ldcg(src_vb + q); }
+      }
+      __syncthreads();
+      // S2: sch = sqrt(ter(ch)) on U, supb
+      for (int pp = tid; pp < (tw + 3) * (th + 3); pp += nth) {
+        PT(tw + 3, 0, 0)
+        double sch = 1.0;
+        if (__ldg(P.lev_u + q) > 0) {
+          const double w = (j <= njm) ? (S(B_CH, p) + S(B_CH, p + W) + S(B_CH, p + 1) + S(B_CH, p + W + 1)) * 0.25 : 0.0;
+          sch = sqrt(w);
+        }
+        const double ps = ld(P.prh_u, q) * sch;
+        S(B_S1, p) = ps * S(B_UB, p);
+        S(B_X2, p) = ps * S(B_VB, p) * __ldg(P.rh1d[3] + j - 1);
+      }
+      __syncthreads();
+      // S4: predictor ch
+      for (int pp = tid; pp < (tw + 2) * (th + 2); pp += nth) {
+        PT(tw + 2, 1, 1)
+        const bool srow = j >= 2;
+        const double tEc = srow ? 0.5 * (S(B_S1, p - W) + S(B_S1, p)) : 0.0;
+        const double tEw = srow ? 0.5 * (S(B_S1, p - W - 1) + S(B_S1, p - 1)) : 0.0;
+        const double A = dvr(tEc - tEw, __ldg(P.dxx1d[1] + i - 1), __ldg(P.rdxx1d[1] + i - 1));
+        double B = 0.0;
+        if (srow) {
+          const double tNc = 0.5 * (S(B_X2, p - 1) + S(B_X2, p));
+          const double tNs = 0.5 * (S(B_X2, p - W - 1) + S(B_X2, p - W));
+          B = dvr(tNc - tNs, __ldg(P.dxy1d[1] + j - 1), __ldg(P.rdxy1d[1] + j - 1));
+        }
+        const double div = dvr(A + B, __ldg(P.arh1d[1] + j - 1), __ldg(P.rarh1d[1] + j - 1));
+        double pred;
+        if (__ldg(P.lev_t + q) > 0) pred = S(B_CH, p) - dvr(div * bt * gamma_b, ld(P.prh_t, q), ld(P.rprh_t, q));
+        else pred = (nt == 1) ? P.chc[q] : S(B_CH, p);
+        S(B_PRED, p) = pred;
+      }
+      __syncthreads();
+      // S5: sch on U, N- and E-grid intermediates
+      for (int pp = tid; pp < (tw + 2) * (th + 2); pp += nth) {
+        PT(tw + 2, 1, 1)
+        const bool nrow = j <= njm, srow = j >= 2;
+        const bool inU = lx < tw + 2 && ly < th + 2, inN = ly < th + 2, inE = lx < tw + 2;
+        if (inU) {
+          double sch = 1.0;
+          if (__ldg(P.lev_u + q) > 0) {
+            const double w = nrow ? (S(B_PRED, p) + S(B_PRED, p + W) + S(B_PRED, p + 1) + S(B_PRED, p + W + 1)) * 0.25 : 0.0;
+            sch = sqrt(w);
+          }
+          S(B_SCHE, p) = sch;
+        }
+        if (inN) {
+          const double dx4 = __ldg(P.dxx1d[4] + i - 1), rdx4 = __ldg(P.rdxx1d[4] + i - 1);
+          const double rh4 = __ldg(P.rh1d[4] + j - 1), rrh4 = __ldg(P.rrh1d[4] + j - 1);
+          S(B_A1U, p) = dvr(dvr(S(B_UB, p) - S(B_UB, p - 1), dx4, rdx4), rh4, rrh4);
+          S(B_A1V, p) = dvr(dvr(S(B_VB, p) - S(B_VB, p - 1), dx4, rdx4), rh4, rrh4);
+          if (nrow) {
+            S(B_GY, p) = dvr(dvr(S(B_PRED, p + W) - S(B_PRED, p), __ldg(P.dxy1d[4] + j - 1), __ldg(P.rdxy1d[4] + j - 1)), a, ra);
+            S(B_CN, p) = 0.5 * (S(B_PRED, p) + S(B_PRED, p + W));
+          } else {
+            S(B_GY, p) = 0.0;
+            S(B_CN, p) = 0.0;
+          }
+        }
+        if (inE) {
+          const double rh2 = __ldg(P.rh1d[2] + j - 1);
+          if (srow) {
+            const double dy2 = __ldg(P.dxy1d[2] + j - 1), rdy2 = __ldg(P.rdxy1d[2] + j - 1);
+            S(B_A2U, p) = dvr(S(B_UB, p) - S(B_UB, p - W), dy2, rdy2) * rh2;
+            S(B_A2V, p) = dvr(S(B_VB, p) - S(B_VB, p - W), dy2, rdy2) * rh2;
+          } else {
+            S(B_A2U, p) = 0.0;
+            S(B_A2V, p) = 0.0;
+          }
+          S(B_GX, p) = dvr(dvr(S(B_PRED, p + 1) - S(B_PRED, p), __ldg(P.dxx1d[2] + i - 1), __ldg(P.rdxx1d[2] + i - 1)),
+                           __ldg(P.arh1d[2] + j - 1), __ldg(P.rarh1d[2] + j - 1));
+          S(B_CE, p) = 0.5 * (S(B_PRED, p) + S(B_PRED, p + 1));
+        }
+      }
+      __syncthreads();
+      // S6: corrector velocity
+      for (int pp = tid; pp < (tw + 1) * (th + 1); pp += nth) {
+        PT(tw + 1, 1, 1)
+        const bool nrow = j <= njm;
+        const double seau = (double)(__ldg(P.lev_u + q) >= 1);
+        const double rh3 = __ldg(P.rh1d[3] + j - 1);
+        const double dx3 = __ldg(P.dxx1d[3] + i - 1), rdx3 = __ldg(P.rdxx1d[3] + i - 1);
+        const double dy3 = __ldg(P.dxy1d[3] + j - 1), rdy3 = __ldg(P.rdxy1d[3] + j - 1);
+        const double aarh = __ldg(P.aarh3 + j - 1), raarh = __ldg(P.raarh3 + j - 1);
+        const double L1u = dvr(S(B_A1U, p + 1) - S(B_A1U, p), dx3, rdx3);
+        const double L1v = dvr(S(B_A1V, p + 1) - S(B_A1V, p), dx3, rdx3);
+        const double L2u = nrow ? dvr(S(B_A2U, p + W) - S(B_A2U, p), dy3, rdy3) : 0.0;
+        const double L2v = nrow ? dvr(S(B_A2V, p + W) - S(B_A2V, p), dy3, rdy3) : 0.0;
+        const double sam1 = seau * ld(P.am, q);
+        const double vsu = sam1 * dvr(L1u + L2u, aarh, raarh);
+        const double vsv = sam1 * dvr(L1v + L2v, aarh, raarh);
+        double dvu, dvv;
+        if (nt == 1) {
+          dvu = vsu - vsu;
+          dvv = vsv - vsv;
+          if (lx >= 2 && ly >= 2) { P.tr_acc[4][q] = vsu; P.tr_acc[5][q] = vsv; }
+        } else {
+          dvu = vsu - __ldcg(P.tr_acc[4] + q);
+          dvv = vsv - __ldcg(P.tr_acc[5] + q);
+        }
+        double gi1 = 0.0, cg1 = 0.0;
+        if (nrow) {
+          gi1 = 0.5 * (S(B_GX, p) * ld(P.bphi[0], q) + S(B_GX, p + W) * ld(P.bphi[1], q + ni));
+          cg1 = 0.5 * (S(B_CE, p) * ld(P.bgra[0], q) + S(B_CE, p + W) * ld(P.bgra[1], q + ni));
+        }
+        const double gi2 = 0.5 * (S(B_GY, p) * ld(P.bphi[2], q) + S(B_GY, p + 1) * ld(P.bphi[3], q + 1));
+        const double cg2 = 0.5 * (S(B_CN, p) * ld(P.bgra[2], q) + S(B_CN, p + 1) * ld(P.bgra[3], q + 1));
+        const double sch = S(B_SCHE, p);
+        const double pg1 = (gi1 + cg1 + ld(P.graphihx, q)) * seau * sch;
+        const double pg2 = (gi2 + cg2 + ld(P.graphihy, q)) * seau * sch;
+        const double cor = ld(P.cor, q), ut = ld(P.ut, q), vt = ld(P.vt, q);
+        const double ubp = S(B_UB, p), vbp = S(B_VB, p);
+        double p1 = seau * (dvu + ut - pg1 + 0.5 * cor * vbp);
+        double p2 = seau * (dvv + vt - pg2 - 0.5 * cor * ubp);
+        const double w1 = p1 * bt + ubp, w2 = p2 * bt + vbp;
+        const double cb = 0.5 * cor * bt;
+        const double den = 1 + cb * cb, rden = ld(P.rwt, q);
+        double u1 = dvr(w1 + 0.5 * cor * bt * w2, den, rden);
+        double v1 = dvr(w2 - 0.5 * cor * bt * w1, den, rden);
+        u1 = 0.5 * (u1 + ubp);
+        v1 = 0.5 * (v1 + vbp);
+        p1 = seau * (dvu - pg1 + ut + cor * v1);
+        p2 = seau * (dvv - pg2 + vt - cor * u1);
+        const double ubc = p1 * bt + ubp, vbc = p2 * bt + vbp;
+        S(B_UBC, p) = ubc;
+        S(B_VBC, p) = vbc;
+        const double ps = ld(P.prh_u, q) * sch;
+        S(B_S1, p) = ps * ubc;
+        S(B_X2, p) = ps * vbc * rh3;
+      }
+      __syncthreads();
+      // S8: corrector ch on the tile, store, accumulate
+      for (int pp = tid; pp < tw * th; pp += nth) {
+        PT(tw, 2, 2)
+        const bool srow = j >= 2;
+        const double tEc = srow ? 0.5 * (S(B_S1, p - W) + S(B_S1, p)) : 0.0;
+        const double tEw = srow ? 0.5 * (S(B_S1, p - W - 1) + S(B_S1, p - 1)) : 0.0;
+        const double A = dvr(tEc - tEw, __ldg(P.dxx1d[1] + i - 1), __ldg(P.rdxx1d[1] + i - 1));
+        double B = 0.0;
+        if (srow) {
+          const double tNc = 0.5 * (S(B_X2, p - 1) + S(B_X2, p));
+          const double tNs = 0.5 * (S(B_X2, p - W - 1) + S(B_X2, p - W));
+          B = dvr(tNc - tNs, __ldg(P.dxy1d[1] + j - 1), __ldg(P.rdxy1d[1] + j - 1));
+        }
+        const double div = dvr(A + B, __ldg(P.arh1d[1] + j - 1), __ldg(P.rarh1d[1] + j - 1));
+        const double m1 = (double)(__ldg(P.lev_t + q) >= 1);
+        const double chn = S(B_CH, p) - dvr(m1 * div * bt, ld(P.prh_t, q), ld(P.rprh_t, q));
+        const double ubc = S(B_UBC, p), vbc = S(B_VBC, p);
+        st2(P.tr_ch[d], P, i, q, chn);
+        st2(P.tr_ub[d], P, i, q, ubc);
+        st2(P.tr_vb[d], P, i, q, vbc);
+        if (nt <= nstep / 2) P.tr_acc[0][q] = P.tr_acc[0][q] + chn;
+        P.tr_acc[1][q] = P.tr_acc[1][q] + chn;
+        P.tr_acc[2][q] = P.tr_acc[2][q] + ubc;
+        P.tr_acc[3][q] = P.tr_acc[3][q] + vbc;
+      }
+#undef PT
+      __syncthreads();
+    }
+    if (!batch_barrier(cnt, (unsigned long long)nt * gridDim.x, err)) return;
+  }
+
+  // averages (mod_int.f90:276-288)
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileRef T = tiles[t];
+    const Dev &P = Ps[T.m];
+    for (int p = tid; p < T.tw * T.th; p += nth) {
+      const int i = T.r0 + p % T.tw + 2, j = T.j0 + p / T.tw;
+      const long long q = I2(P, i, j);
+      const double ub = P.tr_acc[2][q] / (nstep + 1), vb = P.tr_acc[3][q] / (nstep + 1);
+      const double mch = P.tr_acc[0][q] / (nstep / 2 + 1), mch2 = P.tr_acc[1][q] / (nstep + 1);
+      st2(P.ubc, P, i, q, ub);
+      st2(P.vbc, P, i, q, vb);
+      st2(P.ubp, P, i, q, ub);
+      st2(P.vbp, P, i, q, vb);
+      st2(P.mch, P, i, q, mch);
+      st2(P.mch2, P, i, q, mch2);
+      st2(P.chc, P, i, q, mch2);
+      st2(P.chp, P, i, q, mch2);
+      st2(P.acch, P, i, q, P.acch[q] + mch2);
+    }
+  }
+}
+
+size_t trop_batch_smem(int TX, int TY) { return (size_t)B_COUNT * (TX + 4) * (TY + 4) * sizeof(double); }
+
+int trop_batch_max_blocks(int TX, int TY) {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = trop_batch_smem(TX, TY);
+  if (cudaFuncSetAttribute(k_trop_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_batch, 256, smem) != cudaSuccess) return 0;
+  return per * nsm;
+}
+
+cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
+                              unsigned long long *cnt, int *err, cudaStream_t s) {
+  const size_t smem = trop_batch_smem(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(k_trop_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // the barrier counter starts from zero in every launch
+  e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  void *args[] = {(void *)&dPs, (void *)&dtiles, (void *)&ntiles, (void *)&TX, (void *)&TY, (void *)&cnt, (void *)&err};
+  return cudaLaunchCooperativeKernel((const void *)k_trop_batch, dim3(nblocks), dim3(256), args, smem, s);
+}

@@ -865,3 +865,313 @@ void pcom_dev_consts(bool r8, DevConsts &c) { make_consts(r8, c); }
 
 // record a failure for pcom_gpu_last_error from another translation unit
 int pcom_set_error(int code, const char *msg) { return fail(code, "%s", msg); }
+
+// =============================================================== batches
+// Ensemble members and basins of uneven size stepped together: every kernel
+// of the step runs once for all members (grid z = member, Dev per member in
+// device memory) and the barotropic subcycle of all members is one
+// persistent cooperative launch over the work list of their tiles.  The
+// whole step can be captured into CUDA graphs (one per ring-buffer phase).
+struct pcom_batch {
+  std::vector<pcom_handle *> hs;
+  cudaStream_t stream = nullptr;
+  BatchShape shape{};
+  int nstep = 0;
+  // barotropic work list
+  TileRef *dtiles = nullptr;
+  int ntiles = 0, TX = 16, TY = 16, nblocks = 0;
+  unsigned long long *cnt = nullptr;
+  int *err = nullptr;
+  // per-phase device copies of the members' Dev (phase = ring indices)
+  struct DevArray {
+    Dev *d;
+    std::vector<Dev> host;
+  };
+  std::map<int, DevArray> dev_arrays;
+  std::map<int, cudaGraphExec_t> graphs;
+  bool use_graphs = true;
+  std::vector<void *> allocs;
+  ~pcom_batch() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+namespace {
+
+int batch_tiles(pcom_batch *b, int TX, int TY) {
+  std::vector<TileRef> t;
+  for (int m = 0; m < (int)b->hs.size(); ++m) {
+    const pcom_handle *h = b->hs[m];
+    const int G = h->dims.glo_ni, nj = h->nj;
+    for (int j0 = 1; j0 <= nj; j0 += TY)
+      for (int r0 = 0; r0 < G; r0 += TX) t.push_back({m, r0, j0, std::min(TX, G - r0), std::min(TY, nj - j0 + 1)});
+  }
+  if (b->dtiles) { cudaFree(b->dtiles); b->allocs.erase(std::find(b->allocs.begin(), b->allocs.end(), (void *)b->dtiles)); }
+  CK(cudaMalloc(&b->dtiles, t.size() * sizeof(TileRef)));
+  b->allocs.push_back(b->dtiles);
+  CK(cudaMemcpy(b->dtiles, t.data(), t.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
+  b->ntiles = (int)t.size();
+  b->TX = TX;
+  b->TY = TY;
+  const int mb = trop_batch_max_blocks(TX, TY);
+  if (mb <= 0) return fail(PCOM_ERR_ARG, "tile %dx%d does not fit the barotropic batch kernel", TX, TY);
+  b->nblocks = std::min(b->ntiles, mb);
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  return PCOM_OK;
+}
+
+// the ring phase of a member: AB3 ring indices and the tracer buffers in use
+int phase_key(const pcom_handle *h) { return h->ic * 100 + h->ip * 10 + h->ipp + 1000 * (h->itc * 4 + h->itp); }
+
+// the device copy of the members' Dev for ring phase `key`, refreshed when a
+// member's Dev changed since it was uploaded (the array keeps its address, so
+// graphs captured with it stay valid)
+int batch_dev_array(pcom_batch *b, int key, Dev **out) {
+  std::vector<Dev> v;
+  for (pcom_handle *h : b->hs) v.push_back(h->D);
+  auto it = b->dev_arrays.find(key);
+  if (it == b->dev_arrays.end()) {
+    Dev *d = nullptr;
+    CK(cudaMalloc(&d, v.size() * sizeof(Dev)));
+    b->allocs.push_back(d);
+    it = b->dev_arrays.emplace(key, pcom_batch::DevArray{d, {}}).first;
+  }
+  pcom_batch::DevArray &a = it->second;
+  if (a.host.size() != v.size() || memcmp(a.host.data(), v.data(), v.size() * sizeof(Dev)) != 0) {
+    a.host = v;
+    CK(cudaMemcpyAsync(a.d, a.host.data(), v.size() * sizeof(Dev), cudaMemcpyHostToDevice, b->stream));
+  }
+  *out = a.d;
+  return PCOM_OK;
+}
+
+// enqueue the kernels of one step for all members with Dev array dP
+int batch_enqueue(pcom_batch *b, Dev *dP) {
+  const BatchShape &s = b->shape;
+  cudaStream_t st = b->stream;
+  launch_batch(BK_ALPHA_TOBOT, dP, s, 0, st);
+  launch_batch(BK_PGRA2D, dP, s, 0, st);
+  launch_batch(BK_UV2D, dP, s, 0, st);
+  launch_batch(BK_UPWELLING, dP, s, 0, st);
+  launch_batch(BK_READYC3D, dP, s, 0, st);
+  cudaError_t e = launch_trop_batch(dP, b->dtiles, b->ntiles, b->TX, b->TY, b->nblocks, b->cnt, b->err, st);
+  if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "batched barotropic launch: %s", cudaGetErrorString(e));
+  launch_batch(BK_UV2D, dP, s, 2, st);
+  launch_batch(BK_CLIN, dP, s, 0, st);
+  launch_batch(BK_SMAG, dP, s, 0, st);
+  launch_batch(BK_SSH, dP, s, 0, st);
+  launch_batch(BK_UV2D, dP, s, 1, st);
+  launch_batch(BK_UPWELLING, dP, s, 1, st);
+  launch_batch(BK_TS, dP, s, 0, st);
+  CK(cudaGetLastError());
+  return PCOM_OK;
+}
+
+int batch_sync(pcom_batch *b) {
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaGetLastError());
+  int err = 0;
+  CK(cudaMemcpy(&err, b->err, sizeof err, cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(b->err, 0, sizeof(int));
+    return fail(PCOM_ERR_TIMEOUT, "a device-side grid barrier of the batch gave up waiting (bounded spin)");
+  }
+  return PCOM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pcom_gpu_batch_create(pcom_handle *const *hs, int32_t n, pcom_batch **out) {
+  if (!hs || n <= 0 || !out) return fail(PCOM_ERR_ARG, "null argument or empty batch");
+  pcom_batch *b = new pcom_batch();
+  for (int m = 0; m < n; ++m) {
+    pcom_handle *h = hs[m];
+    if (!h || !h->static_ok) { delete b; return fail(PCOM_ERR_STATE, "batch member %d has no static data", m); }
+    if (!h->D.separable) { delete b; return fail(PCOM_ERR_ARG, "batch member %d: batches need lat-lon (separable) metrics", m); }
+    if (h->D.bt != hs[0]->D.bt || h->D.bc != hs[0]->D.bc) { delete b; return fail(PCOM_ERR_ARG, "batch members must share dtbt and dtbc"); }
+    if (h->device != hs[0]->device) { delete b; return fail(PCOM_ERR_ARG, "batch members must live on one device"); }
+    b->hs.push_back(h);
+    b->shape.glo_ni = std::max(b->shape.glo_ni, h->dims.glo_ni);
+    b->shape.ni = std::max(b->shape.ni, h->ni);
+    b->shape.nj = std::max(b->shape.nj, h->nj);
+    b->shape.nk = std::max(b->shape.nk, h->nk);
+    cudaStreamSynchronize(h->stream);
+  }
+  b->shape.n = n;
+  b->stream = hs[0]->stream;
+  b->nstep = hs[0]->D.nstep;
+  cudaError_t e = cudaMalloc(&b->cnt, sizeof(unsigned long long));
+  if (e == cudaSuccess) { b->allocs.push_back(b->cnt); e = cudaMalloc(&b->err, sizeof(int)); }
+  if (e == cudaSuccess) { b->allocs.push_back(b->err); e = cudaMemset(b->err, 0, sizeof(int)); }
+  if (e != cudaSuccess) { delete b; return fail(PCOM_ERR_CUDA, "batch scratch: %s", cudaGetErrorString(e)); }
+  int rc = batch_tiles(b, 16, 16);
+  if (rc) { delete b; return rc; }
+  *out = b;
+  return PCOM_OK;
+}
+
+int pcom_gpu_batch_destroy(pcom_batch *b) {
+  if (!b) return PCOM_OK;
+  cudaStreamSynchronize(b->stream);
+  delete b;
+  return PCOM_OK;
+}
+
+int pcom_gpu_batch_use_graphs(pcom_batch *b, int32_t enable) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  b->use_graphs = enable != 0;
+  return PCOM_OK;
+}
+
+int pcom_gpu_batch_den_prho(pcom_batch *b) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  Dev *dP = nullptr;
+  int rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
+  if (rc) return rc;
+  for (pcom_handle *h : b->hs) h->launches++;
+  launch_batch(BK_DEN_PRHO, dP, b->shape, 0, b->stream);
+  return batch_sync(b);
+}
+
+int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  if (tctr_i < 1) return fail(PCOM_ERR_ARG, "tctr_i must be >= 1");
+  // AB3 ring rotation of every member (mod_int.f90:115-118), in lock step
+  const int key0 = phase_key(b->hs[0]);
+  for (pcom_handle *h : b->hs) {
+    if (phase_key(h) != key0) return fail(PCOM_ERR_STATE, "batch members are not in the same ring phase");
+    int old_pp = h->ipp;
+    h->ipp = h->ip;
+    h->ip = h->ic;
+    h->ic = old_pp;
+    bind_rotating(h);
+    const bool fresh = h->dims.rst != 1;
+    h->D.ab3_mode = (fresh && tctr_i == 1) ? 1 : 0;
+  }
+  const bool startup = tctr_i <= 2;
+  for (pcom_handle *h : b->hs)
+    if (h->dims.rst != 1 && tctr_i == 2) {
+      CK(cudaMemcpyAsync(h->D.aupp, h->D.aup, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+      CK(cudaMemcpyAsync(h->D.avpp, h->D.avp, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
+    }
+  const int key = phase_key(b->hs[0]);
+  Dev *dP = nullptr;
+  int rc = batch_dev_array(b, key, &dP);
+  if (rc) return rc;
+  if (startup || !b->use_graphs) {
+    // the start-up steps (ab3_mode, aupp = aup) run kernel by kernel
+    rc = batch_enqueue(b, dP);
+  } else {
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t ge = nullptr;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      rc = batch_enqueue(b, dP);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "graph capture of the batched step: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(e));
+      it = b->graphs.emplace(key, ge).first;
+    }
+    CK(cudaGraphLaunch(it->second, b->stream));
+  }
+  if (rc) return rc;
+  for (pcom_handle *h : b->hs) {
+    h->D.ab3_mode = 0;
+    h->launches += 14;
+    h->n_ch++; h->n_uv++; h->n_ssh++; h->n_w++; h->n_ts++;
+    // tc = tp = the buffer int_ts wrote (mod_int.f90:496-497)
+    int fr = 0;
+    while (fr == h->itc || fr == h->itp) ++fr;
+    h->itc = h->itp = fr;
+    bind_rotating(h);
+  }
+  return PCOM_OK;
+}
+
+int pcom_gpu_batch_sync(pcom_batch *b) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  return batch_sync(b);
+}
+
+int pcom_gpu_batch_step(pcom_batch *b, int64_t tctr_i) {
+  int rc = pcom_gpu_batch_step_async(b, tctr_i);
+  if (rc) return rc;
+  return batch_sync(b);
+}
+
+// Autotuner: time the batched barotropic kernel for candidate tile shapes on
+// the members' current state (the 2-D state it changes is saved and
+// restored around every trial) and keep the fastest.
+int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  static const int cand[][2] = {{8, 8}, {16, 8}, {16, 16}, {24, 18}, {32, 8}, {32, 16}, {32, 24}, {48, 16}, {64, 8}};
+  // save the 2-D fields the subcycle writes
+  std::vector<double *> saved;
+  auto fields = [](pcom_handle *h) {
+    return std::vector<double *>{h->D.chc, h->D.chp, h->D.mch, h->D.mch2, h->D.ubc, h->D.vbc, h->D.ubp, h->D.vbp, h->D.acch};
+  };
+  for (pcom_handle *h : b->hs)
+    for (double *f : fields(h)) {
+      double *c = nullptr;
+      CK(cudaMalloc(&c, h->n2 * sizeof(double)));
+      CK(cudaMemcpy(c, f, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice));
+      saved.push_back(c);
+    }
+  auto restore = [&]() -> int {
+    size_t q = 0;
+    for (pcom_handle *h : b->hs)
+      for (double *f : fields(h)) { CK(cudaMemcpy(f, saved[q], h->n2 * sizeof(double), cudaMemcpyDeviceToDevice)); ++q; }
+    return PCOM_OK;
+  };
+  Dev *dP = nullptr;
+  int rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
+  double best = 1e30;
+  int bx = b->TX, by = b->TY;
+  std::string rep;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (auto &c : cand) {
+    if (rc) break;
+    if (trop_batch_max_blocks(c[0], c[1]) <= 0) continue;
+    rc = batch_tiles(b, c[0], c[1]);
+    if (rc) break;
+    float ms = 0.f, tot = 0.f;
+    for (int rep_i = 0; rep_i < 3 && !rc; ++rep_i) {
+      cudaEventRecord(e0, b->stream);
+      cudaError_t e = launch_trop_batch(dP, b->dtiles, b->ntiles, b->TX, b->TY, b->nblocks, b->cnt, b->err, b->stream);
+      cudaEventRecord(e1, b->stream);
+      if (e != cudaSuccess) rc = fail(PCOM_ERR_CUDA, "autotune launch: %s", cudaGetErrorString(e));
+      if (!rc) rc = batch_sync(b);
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep_i > 0) tot += ms;
+      if (!rc) rc = restore();
+    }
+    const double t = tot / 2.0;
+    char line[96];
+    snprintf(line, sizeof line, "%dx%d:%.3fms(%d tiles,%d CTAs) ", c[0], c[1], t, b->ntiles, b->nblocks);
+    rep += line;
+    if (!rc && t < best) { best = t; bx = c[0]; by = c[1]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (double *c : saved) cudaFree(c);
+  if (rc) return rc;
+  rc = batch_tiles(b, bx, by);
+  if (rc) return rc;
+  char line[96];
+  snprintf(line, sizeof line, "-> %dx%d", bx, by);
+  rep += line;
+  if (report && len > 0) { strncpy(report, rep.c_str(), (size_t)len - 1); report[len - 1] = 0; }
+  return PCOM_OK;
+}
+
+}  // extern "C"

@@ -436,6 +436,49 @@ int pcom_model_run(pcom_model *M, int64_t nsteps) {
   return PCOM_OK;
 }
 
+int pcom_model_run_batch(pcom_model *const *ms, int32_t n, pcom_batch *b, int64_t nsteps) {
+  if (!ms || n <= 0 || !b) return PCOM_ERR_ARG;
+  for (int m = 0; m < n; ++m) {
+    if (!ms[m] || !ms[m]->h) return PCOM_ERR_STATE;
+    const pcom_model &A = *ms[m], &B = *ms[0];
+    if (A.iter != B.iter || A.bc != B.bc || A.ct.y != B.ct.y || A.ct.m != B.ct.m || A.ct.d != B.ct.d || A.ct.h != B.ct.h)
+      return PCOM_ERR_STATE;
+  }
+  for (int64_t s = 0; s < nsteps; ++s) {
+    pcom_model &M0 = *ms[0];
+    const bool day = M0.iter + 1 == 1 || M0.ct.d != M0.pt.d;
+    if (day) {
+      // the members' forcing buffers are rewritten: wait for the batch first
+      int rc = pcom_gpu_batch_sync(b);
+      if (rc) return rc;
+    }
+    for (int m = 0; m < n; ++m) {
+      pcom_model &M = *ms[m];
+      M.iter += 1;
+      if (day) {
+        int_bnd(M);
+        M.nday += 1;
+        pcom_forcing f{M.bnd[0].v.data(), M.bnd[1].v.data(), M.bnd[2].v.data(),
+                       M.bnd[3].v.data(), M.bnd[4].v.data(), M.bnd[5].v.data()};
+        int rc = pcom_gpu_set_forcing(M.h, &f);
+        if (rc) return rc;
+      }
+    }
+    if (day) {
+      int rc = pcom_gpu_batch_den_prho(b);
+      if (rc) return rc;
+    }
+    int rc = pcom_gpu_batch_step_async(b, M0.iter);
+    if (rc) return rc;
+    for (int m = 0; m < n; ++m) {
+      pcom_model &M = *ms[m];
+      M.pt = M.ct;
+      M.ct = advance(M.ct, M.bc);
+    }
+  }
+  return pcom_gpu_batch_sync(b);
+}
+
 int64_t pcom_model_iter(pcom_model *m) { return m ? m->iter : -1; }
 
 int pcom_model_date(pcom_model *m, int32_t *ymdh4) {

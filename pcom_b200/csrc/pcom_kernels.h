@@ -14,6 +14,16 @@ void launch_ssh(const Dev &P, cudaStream_t s);
 void launch_ts(const Dev &P, cudaStream_t s);
 void launch_den_prho(const Dev &P, cudaStream_t s);
 
+// batched forms: member m = blockIdx.z reads its Dev from dPs[m]
+struct BatchShape {
+  int n;                      // members
+  int glo_ni, ni, nj, nk;     // the largest extents over the members
+};
+enum {
+  BK_ALPHA_TOBOT, BK_PGRA2D, BK_UV2D, BK_UPWELLING, BK_READYC3D, BK_CLIN, BK_SMAG, BK_SSH, BK_TS, BK_DEN_PRHO
+};
+void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cudaStream_t s);
+
 size_t trop_smem_bytes(int TX, int TY);
 cudaError_t launch_trop(const Dev &P, int TX, int TY, int nblocks, cudaStream_t s);
 int trop_max_blocks(int TX, int TY);
@@ -26,6 +36,15 @@ int trop_res_max_blocks(int TX, int TY);
 size_t trop_fast_smem_bytes(int TX, int TY);
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
 int trop_fast_max_blocks(int TX, int TY);
+
+// batched barotropic subcycle: one persistent launch over the tiles of all members
+struct TileRef {
+  int m, r0, j0, tw, th;  // member, first interior ring column (0-based), first row, width, height
+};
+size_t trop_batch_smem(int TX, int TY);
+int trop_batch_max_blocks(int TX, int TY);
+cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
+                              unsigned long long *cnt, int *err, cudaStream_t s);
 
 // the model constants (literal precision per PCOM_LIT_R8)
 void pcom_dev_consts(bool r8, DevConsts &c);

@@ -182,3 +182,53 @@ class Model:
 
     def launch_count(self) -> int:
         return int(self.lib.pcom_gpu_launch_count(self.handle))
+
+
+class Batch:
+    """Several models stepped together on one device (ensemble members and
+    basins of uneven size sharing dtbt, dtbc and the start date): each
+    kernel of the step runs once for all members, the barotropic subcycles
+    of all members are one persistent launch, and after the two start-up
+    steps the batched step replays from captured CUDA graphs."""
+
+    def __init__(self, models: list[Model], graphs: bool = True):
+        self.lib = L.load()
+        self.models = list(models)
+        n = len(self.models)
+        hs = (C.c_void_p * n)(*[m.handle.value for m in self.models])
+        self._b = C.c_void_p()
+        L.check(self.lib.pcom_gpu_batch_create(hs, n, C.byref(self._b)), "pcom_gpu_batch_create")
+        self._ms = (C.c_void_p * n)(*[m._m.value for m in self.models])
+        self.use_graphs(graphs)
+
+    def use_graphs(self, on: bool):
+        L.check(self.lib.pcom_gpu_batch_use_graphs(self._b, 1 if on else 0), "batch_use_graphs")
+
+    def run(self, nsteps: int = 1):
+        L.check(self.lib.pcom_model_run_batch(self._ms, len(self.models), self._b, int(nsteps)),
+                "pcom_model_run_batch")
+
+    def step_async(self, tctr_i: int):
+        L.check(self.lib.pcom_gpu_batch_step_async(self._b, int(tctr_i)), "batch_step_async")
+
+    def den_prho(self):
+        L.check(self.lib.pcom_gpu_batch_den_prho(self._b), "batch_den_prho")
+
+    def sync(self):
+        L.check(self.lib.pcom_gpu_batch_sync(self._b), "batch_sync")
+
+    def autotune(self) -> str:
+        buf = C.create_string_buffer(1024)
+        L.check(self.lib.pcom_gpu_batch_autotune(self._b, buf, 1024), "batch_autotune")
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            self.lib.pcom_gpu_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
