@@ -49,6 +49,12 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="global1", choices=["global1", "ensemble"],
+                   help="ensemble: 32 perturbed 1-degree members + 16 uneven basins, batched")
+    p.add_argument("--members", type=int, default=32)
+    p.add_argument("--member-case", default="box", choices=["box", "global1"],
+                   help="ensemble member grid: box 128x64x20 or the 1-degree 360x160x30 case")
+    p.add_argument("--basins", type=int, default=16)
     return p.parse_args()
 
 
@@ -312,6 +318,169 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def ensemble_cases(members: int, basins: int, member_case: str = "box"):
+    """Members of one case (default the 128x64x20 1-degree box) with seeded
+    N(0, 0.05 K) perturbations of T (seeds 1..members), and idealized basins
+    from 64x32 to 256x128 with 20 to 30 levels (all with dtbt 60 s, dtbc
+    3600 s)."""
+    from pcom_b200.synth import make_case, perturb
+
+    base = make_case(member_case)
+    cases = [perturb(base, m + 1, 0.05) for m in range(members)]
+    for b in range(basins):
+        f = b / max(basins - 1, 1)
+        ni = int(round((64 + 192 * f) / 8)) * 8
+        cases.append(make_case("basin", seed=100 + b, glo_ni=ni, glo_nj=ni // 2, nk=int(round(20 + 10 * f))))
+    return cases
+
+
+def run_ensemble(args):
+    """Aggregate SYPD of a batched ensemble vs the same members stepped one
+    after another through the single-domain path (same stream, same models)."""
+    import ctypes as C
+
+    import torch
+
+    from pcom_b200 import _lib as L
+    from pcom_b200.model import Batch, Model
+
+    torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    cases = ensemble_cases(args.members, args.basins, args.member_case)
+    stream = torch.cuda.current_stream()
+    models = []
+    for c in cases:
+        m = Model(c)
+        m.set_stream(stream.cuda_stream)
+        models.append(m)
+    lib = models[0].lib
+    n = len(models)
+    b = Batch(models)
+    warm = max(args.warmup, 3)
+    b.run(warm)  # AB3 start-up steps
+    tune = b.autotune()
+    b.run(3)  # capture the graph of every ring phase
+    it0 = models[0].iter
+    day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
+    steps = args.steps
+
+    def timed(body):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        body()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    counts0 = b.launch_count()
+
+    def batched(first):
+        def body():
+            for q in range(steps):
+                it = first + q
+                if day_of(it) != day_of(it - 1):
+                    b.den_prho()
+                b.step_async(it)
+        return body
+
+    with Clocks(dev) as clk:
+        t_batch = timed(batched(it0 + 1))
+    b.sync()
+    launches_batched = b.launch_count() - counts0
+
+    def sequential(first):
+        def body():
+            for q in range(steps):
+                it = first + q
+                for m in models:
+                    if day_of(it) != day_of(it - 1):
+                        L.check(lib.pcom_gpu_den_prho(m.handle), "den_prho")
+                    L.check(lib.pcom_gpu_step_async(m.handle, it), "step")
+        return body
+
+    t_seq = timed(sequential(it0 + 1 + steps))
+    for m in models:
+        m.sync()
+
+    # e2e through the public API: per step every member's forcing from pinned
+    # host memory, the batched step, and every member's barotropic state back
+    pin = lambda k: torch.empty(k, dtype=torch.float64, pin_memory=True)
+    dp = lambda t_: C.cast(t_.data_ptr(), L.dbl_p)
+    fos, sts, keep = [], [], []
+    h2d = d2h = 0
+    for m in models:
+        n2 = m.ni * m.nj
+        hf = m.int_bnd()
+        frc = [pin(n2) for _ in range(6)]
+        for t_, k_ in zip(frc, ("taux", "tauy", "t", "s", "pa", "fw")):
+            t_.copy_(torch.from_numpy(hf[k_].reshape(-1)))
+        out = [pin(n2) for _ in range(3)]
+        keep += frc + out
+        fos.append(L.Forcing(*[dp(t_) for t_ in frc]))
+        st = L.State(*[None] * len(L.STATE_FIELDS))
+        st.chc, st.ubc, st.vbc = dp(out[0]), dp(out[1]), dp(out[2])
+        sts.append(st)
+        h2d += 6 * n2 * 8
+        d2h += 3 * n2 * 8
+    first = it0 + 1 + 2 * steps
+
+    def e2e_body():
+        for q in range(steps):
+            it = first + q
+            for m, fo in zip(models, fos):
+                L.check(lib.pcom_gpu_set_forcing(m.handle, C.byref(fo)), "set_forcing")
+            if day_of(it) != day_of(it - 1):
+                b.den_prho()
+            b.step_async(it)
+            b.sync()
+            for m, st in zip(models, sts):
+                L.check(lib.pcom_gpu_get_state(m.handle, C.byref(st)), "get_state")
+
+    t_e2e = timed(e2e_body)
+    for m in models:
+        L.check(lib.pcom_gpu_check_finite(m.handle), "watchdog")
+
+    ms_b, ms_s, ms_e = t_batch / steps, t_seq / steps, t_e2e / steps
+    member_desc = {"box": "128x64x20 1-degree box", "global1": "360x160x30 1-degree near-global"}[args.member_case]
+    clocks = clk.summary()
+    line = {
+        "metric": "aggregate SYPD of a batched ensemble (sum over members), FP64 plain path",
+        "value": round(n * sypd(ms_b / 1000.0), 2),
+        "unit": "SYPD",
+        "n_gpus": 1,
+        "steps": steps,
+        "warmup": warm + 3,
+        "ms_per_step": round(ms_b, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring; seeded T perturbations)",
+        "config": {
+            "workload": f"ensemble: {args.members} members of the {member_desc} case (T + N(0, 0.05 K), "
+                        f"seeds 1..{args.members}) + {args.basins} basins 64x32..256x128 with 20-30 levels, "
+                        "dtbc 3600 s, dtbt 60 s, one batched step per step",
+            "members": n,
+            "parallelism": "single GPU, batched (grid z = member; one persistent barotropic launch)",
+            "l2": "inputs larger than L2: the members' state is tens of GB",
+            "autotune": tune,
+        },
+        "sequential": {"ms_per_step": round(ms_s, 4), "value": round(n * sypd(ms_s / 1000.0), 2),
+                       "speedup": round(ms_s / ms_b, 3)},
+        "e2e": {"value": round(n * sypd(ms_e / 1000.0), 2), "unit": "SYPD", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches_batched),
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line))
+    b.close()
+    for m in models:
+        m.close()
+
+
 def cpu_baseline(nsteps: int):
     """The oracle (C++ restatement, OpenMP over all host threads) on a bounded
     sample of the same workload: nsteps steps of the 360x160x30 case."""
@@ -366,5 +535,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "ensemble":
+        run_ensemble(a)
     else:
         run_ours(a)

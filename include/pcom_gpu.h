@@ -188,6 +188,12 @@ int pcom_gpu_batch_use_graphs(pcom_batch *b, int32_t enable);
  * members' current state (which it saves and restores) and keep the fastest;
  * a one-line report of the trials goes to `report`. */
 int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len);
+/* Set the barotropic tile shape by hand (tx, ty >= 1, (tx+4)*(ty+4) <= 640)
+ * and optionally cap the tiles of one co-resident group (max_resident > 0;
+ * members with more tiles use the multi-tile kernel).  0 = no cap. */
+int pcom_gpu_batch_set_tiles(pcom_batch *b, int32_t tx, int32_t ty, int32_t max_resident);
+/* Kernels the batch has launched (graph replays included). */
+int64_t pcom_gpu_batch_launch_count(pcom_batch *b);
 
 /* --- allocation-free barotropic subcycle -------------------------------- */
 /* No counterpart in the reference.  One int_trop subcycle (the same kernel

@@ -107,6 +107,8 @@ SIGNATURES = {
     "pcom_gpu_batch_step_async": (C.c_int, [C.c_void_p, C.c_int64]),
     "pcom_gpu_batch_den_prho": (C.c_int, [C.c_void_p]),
     "pcom_gpu_batch_sync": (C.c_int, [C.c_void_p]),
+    "pcom_gpu_batch_set_tiles": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "pcom_gpu_batch_launch_count": (C.c_int64, [C.c_void_p]),
     "pcom_gpu_batch_use_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "pcom_model_create": (C.c_int, [C.POINTER(Case), C.c_int32, C.POINTER(C.c_void_p)]),

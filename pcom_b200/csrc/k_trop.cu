@@ -673,9 +673,20 @@ int trop_res_max_blocks(int TX, int TY) {
 // correctly rounded reciprocal (dvr), which removes the per-division
 // reciprocal-approximation instruction from the critical path.
 
+//
+// GROUP = true: the same kernel over a work list of tiles of several domains
+// (ensemble members, basins), one tile per CTA; each CTA reads its domain's
+// Dev from `Ps`, and the grid barrier counts on `gcnt` (zeroed before the
+// launch) with timeouts flagged in `gerr`.
+template <bool GROUP>
 __global__ void __launch_bounds__(kResThreads, 1)
-    k_trop_fast(const __grid_constant__ Dev P, int TX, int TY, int ntx, unsigned long long epoch) {
+    k_trop_fast(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, const TileRef *__restrict__ tiles,
+                int TX, int TY, int ntx, unsigned long long epoch, unsigned long long *gcnt, int *gerr) {
   extern __shared__ double sm[];
+  const TileRef T = GROUP ? tiles[blockIdx.x] : TileRef{0, 0, 0, 0, 0};
+  const Dev &P = GROUP ? Ps[T.m] : P0;
+  unsigned long long *const bar_cnt = GROUP ? gcnt : P.tile_flag;
+  int *const bar_err = GROUP ? gerr : P.err;
   const int ni = P.ni, nj = P.nj, njm = P.njm, G = P.glo_ni;
   const int W = TX + 4, H = TY + 4, RS = W * H;
   double *vx = sm + R_COUNT * RS;  // dxx[1..4], 1/dxx[1..4] over lx: 8*W
@@ -683,9 +694,14 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const double a = P.c.a, bt = (double)P.bt, gamma_b = P.c.gamma_b;
   const int nstep = P.nstep;
   const int tid = threadIdx.x;
-  const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
-  const int R0 = tx * TX, J0 = ty * TY + 1;
-  const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+  int R0, J0, tw, th;
+  if (GROUP) {
+    R0 = T.r0; J0 = T.j0; tw = T.tw; th = T.th;
+  } else {
+    const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+    R0 = tx * TX; J0 = ty * TY + 1;
+    tw = min(TX, G - R0); th = min(TY, nj - J0 + 1);
+  }
   const int rr0 = R0 - 2, jj0 = J0 - 2;
   auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
 
@@ -912,10 +928,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
     __syncthreads();
     if (tid == 0) {
       __threadfence();
-      atomicAdd(P.tile_flag, 1ULL);
+      atomicAdd(bar_cnt, 1ULL);
       const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
-      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*P.tile_flag);
-      cuda::atomic_ref<int, cuda::thread_scope_device> err(P.err[0]);
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*bar_cnt);
+      cuda::atomic_ref<int, cuda::thread_scope_device> err(bar_err[0]);
       long long it = 0;
       while (c.load(cuda::memory_order_acquire) < want) {
         if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
@@ -926,7 +942,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
       }
     }
     __syncthreads();
-    if (*(volatile int *)P.err != 0) return;
+    if (*(volatile int *)bar_err != 0) return;
   }
   if (inS8) {
     const double ub = acc_u / (nstep + 1), vb = acc_v / (nstep + 1);
@@ -951,20 +967,50 @@ size_t trop_fast_smem_bytes(int TX, int TY) {
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
   const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  cudaError_t e = cudaFuncSetAttribute(k_trop_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_trop_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
-  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch};
-  return cudaLaunchCooperativeKernel((const void *)k_trop_fast, dim3(ntx * nty), dim3(nthreads), args, smem, s);
+  const Dev *nps = nullptr;
+  const TileRef *nts = nullptr;
+  unsigned long long *ncnt = nullptr;
+  int *nerr = nullptr;
+  void *args[] = {(void *)&P, (void *)&nps, (void *)&nts, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch,
+                  (void *)&ncnt, (void *)&nerr};
+  return cudaLaunchCooperativeKernel((const void *)k_trop_fast<false>, dim3(ntx * nty), dim3(nthreads), args, smem, s);
 }
 
-int trop_fast_max_blocks(int TX, int TY) {
+namespace {
+template <bool GROUP>
+int fast_max_blocks(int TX, int TY) {
   int dev = 0, nsm = 0, per = 0;
+  if ((TX + 4) * (TY + 4) > kResThreads) return 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  if (cudaFuncSetAttribute(k_trop_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  if (cudaFuncSetAttribute(k_trop_fast<GROUP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 0;
   const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_fast, nthreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_fast<GROUP>, nthreads, smem) != cudaSuccess) return 0;
   return per * nsm;
+}
+}  // namespace
+
+int trop_fast_max_blocks(int TX, int TY) { return fast_max_blocks<false>(TX, TY); }
+int trop_group_max_blocks(int TX, int TY) { return fast_max_blocks<true>(TX, TY); }
+
+cudaError_t launch_trop_group(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY,
+                              unsigned long long *cnt, int *err, cudaStream_t s) {
+  const size_t smem = trop_fast_smem_bytes(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(k_trop_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // the group's barrier counter starts from zero in every launch
+  e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
+  Dev none{};
+  const int ntx = 0;
+  const unsigned long long epoch = 0;
+  void *args[] = {(void *)&none, (void *)&dPs, (void *)&dtiles, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch,
+                  (void *)&cnt, (void *)&err};
+  return cudaLaunchCooperativeKernel((const void *)k_trop_fast<true>, dim3(ntiles), dim3(nthreads), args, smem, s);
 }

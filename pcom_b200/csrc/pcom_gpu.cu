@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -874,12 +875,25 @@ int pcom_set_error(int code, const char *msg) { return fail(code, "%s", msg); }
 // whole step can be captured into CUDA graphs (one per ring-buffer phase).
 struct pcom_batch {
   std::vector<pcom_handle *> hs;
+  // the batch's own stream (capturable), joined by events to the members'
+  // streams before and after its work
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<cudaStream_t> member_streams;
   BatchShape shape{};
   int nstep = 0;
-  // barotropic work list
-  TileRef *dtiles = nullptr;
-  int ntiles = 0, TX = 16, TY = 16, nblocks = 0;
+  // barotropic work: members packed into groups whose tiles are co-resident
+  // (one tile per CTA, the fast kernel over a tile list); members too large
+  // to be resident go to one group of the multi-tile kernel
+  struct TropGroup {
+    TileRef *d;
+    int ntiles, nblocks;
+    bool resident;
+  };
+  std::vector<TropGroup> groups;
+  int TX = 24, TY = 18;
+  int max_resident = 0;  // > 0: cap on the tiles of one resident group
+  int64_t launches = 0;  // kernels this batch launched
   unsigned long long *cnt = nullptr;
   int *err = nullptr;
   // per-phase device copies of the members' Dev (phase = ring indices)
@@ -894,31 +908,104 @@ struct pcom_batch {
   ~pcom_batch() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
     for (void *p : allocs) cudaFree(p);
+    if (ev) cudaEventDestroy(ev);
+    if (stream) cudaStreamDestroy(stream);
   }
 };
 
 namespace {
 
+void member_tiles(const pcom_handle *h, int m, int TX, int TY, std::vector<TileRef> &t) {
+  const int G = h->dims.glo_ni, nj = h->nj;
+  for (int j0 = 1; j0 <= nj; j0 += TY)
+    for (int r0 = 0; r0 < G; r0 += TX) t.push_back({m, r0, j0, std::min(TX, G - r0), std::min(TY, nj - j0 + 1)});
+}
+
+// plan the barotropic launches for tile shape TX x TY: first-fit decreasing
+// packing of the members' tile lists into groups of at most `cap` tiles
 int batch_tiles(pcom_batch *b, int TX, int TY) {
-  std::vector<TileRef> t;
-  for (int m = 0; m < (int)b->hs.size(); ++m) {
-    const pcom_handle *h = b->hs[m];
-    const int G = h->dims.glo_ni, nj = h->nj;
-    for (int j0 = 1; j0 <= nj; j0 += TY)
-      for (int r0 = 0; r0 < G; r0 += TX) t.push_back({m, r0, j0, std::min(TX, G - r0), std::min(TY, nj - j0 + 1)});
+  for (pcom_batch::TropGroup &g : b->groups) {
+    cudaFree(g.d);
+    b->allocs.erase(std::find(b->allocs.begin(), b->allocs.end(), (void *)g.d));
   }
-  if (b->dtiles) { cudaFree(b->dtiles); b->allocs.erase(std::find(b->allocs.begin(), b->allocs.end(), (void *)b->dtiles)); }
-  CK(cudaMalloc(&b->dtiles, t.size() * sizeof(TileRef)));
-  b->allocs.push_back(b->dtiles);
-  CK(cudaMemcpy(b->dtiles, t.data(), t.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
-  b->ntiles = (int)t.size();
-  b->TX = TX;
-  b->TY = TY;
-  const int mb = trop_batch_max_blocks(TX, TY);
-  if (mb <= 0) return fail(PCOM_ERR_ARG, "tile %dx%d does not fit the barotropic batch kernel", TX, TY);
-  b->nblocks = std::min(b->ntiles, mb);
+  b->groups.clear();
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  int cap = trop_group_max_blocks(TX, TY);
+  if (b->max_resident > 0) cap = std::min(cap, b->max_resident);
+  const int n = (int)b->hs.size();
+  std::vector<std::vector<TileRef>> mt(n);
+  for (int m = 0; m < n; ++m) member_tiles(b->hs[m], m, TX, TY, mt[m]);
+  std::vector<int> order(n);
+  for (int m = 0; m < n; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return mt[x].size() > mt[y].size(); });
+  std::vector<std::vector<TileRef>> res;  // resident groups
+  std::vector<TileRef> big;               // members that cannot be resident
+  for (int m : order) {
+    const int nt = (int)mt[m].size();
+    if (nt > cap) {
+      big.insert(big.end(), mt[m].begin(), mt[m].end());
+      continue;
+    }
+    bool placed = false;
+    for (auto &g : res)
+      if ((int)(g.size() + nt) <= cap) {
+        g.insert(g.end(), mt[m].begin(), mt[m].end());
+        placed = true;
+        break;
+      }
+    if (!placed) res.push_back(mt[m]);
+  }
+  auto add = [&](const std::vector<TileRef> &t, bool resident) -> int {
+    pcom_batch::TropGroup g{nullptr, (int)t.size(), 0, resident};
+    CK(cudaMalloc(&g.d, t.size() * sizeof(TileRef)));
+    b->allocs.push_back(g.d);
+    CK(cudaMemcpy(g.d, t.data(), t.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
+    if (resident) {
+      g.nblocks = g.ntiles;
+    } else {
+      const int mb = trop_batch_max_blocks(TX, TY);
+      if (mb <= 0) return fail(PCOM_ERR_ARG, "tile %dx%d does not fit the multi-tile barotropic kernel", TX, TY);
+      g.nblocks = std::min(g.ntiles, mb);
+    }
+    b->groups.push_back(g);
+    return PCOM_OK;
+  };
+  for (auto &g : res) {
+    int rc = add(g, true);
+    if (rc) return rc;
+  }
+  if (!big.empty()) {
+    int rc = add(big, false);
+    if (rc) return rc;
+  }
+  b->TX = TX;
+  b->TY = TY;
+  return PCOM_OK;
+}
+
+// the barotropic subcycles of all members
+cudaError_t batch_trop(pcom_batch *b, const Dev *dP) {
+  for (const pcom_batch::TropGroup &g : b->groups) {
+    cudaError_t e = g.resident ? launch_trop_group(dP, g.d, g.ntiles, b->TX, b->TY, b->cnt, b->err, b->stream)
+                               : launch_trop_batch(dP, g.d, g.ntiles, b->TX, b->TY, g.nblocks, b->cnt, b->err, b->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// order the batch's stream after the work enqueued on the members' streams
+int batch_join_in(pcom_batch *b) {
+  for (cudaStream_t s : b->member_streams) {
+    CK(cudaEventRecord(b->ev, s));
+    CK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  return PCOM_OK;
+}
+// and the members' streams after the batch's work
+int batch_join_out(pcom_batch *b) {
+  CK(cudaEventRecord(b->ev, b->stream));
+  for (cudaStream_t s : b->member_streams) CK(cudaStreamWaitEvent(s, b->ev, 0));
   return PCOM_OK;
 }
 
@@ -956,7 +1043,7 @@ int batch_enqueue(pcom_batch *b, Dev *dP) {
   launch_batch(BK_UV2D, dP, s, 0, st);
   launch_batch(BK_UPWELLING, dP, s, 0, st);
   launch_batch(BK_READYC3D, dP, s, 0, st);
-  cudaError_t e = launch_trop_batch(dP, b->dtiles, b->ntiles, b->TX, b->TY, b->nblocks, b->cnt, b->err, st);
+  cudaError_t e = batch_trop(b, dP);
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "batched barotropic launch: %s", cudaGetErrorString(e));
   launch_batch(BK_UV2D, dP, s, 2, st);
   launch_batch(BK_CLIN, dP, s, 0, st);
@@ -1002,13 +1089,17 @@ int pcom_gpu_batch_create(pcom_handle *const *hs, int32_t n, pcom_batch **out) {
     cudaStreamSynchronize(h->stream);
   }
   b->shape.n = n;
-  b->stream = hs[0]->stream;
   b->nstep = hs[0]->D.nstep;
-  cudaError_t e = cudaMalloc(&b->cnt, sizeof(unsigned long long));
+  for (pcom_handle *h : b->hs)
+    if (std::find(b->member_streams.begin(), b->member_streams.end(), h->stream) == b->member_streams.end())
+      b->member_streams.push_back(h->stream);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->cnt, sizeof(unsigned long long));
   if (e == cudaSuccess) { b->allocs.push_back(b->cnt); e = cudaMalloc(&b->err, sizeof(int)); }
   if (e == cudaSuccess) { b->allocs.push_back(b->err); e = cudaMemset(b->err, 0, sizeof(int)); }
   if (e != cudaSuccess) { delete b; return fail(PCOM_ERR_CUDA, "batch scratch: %s", cudaGetErrorString(e)); }
-  int rc = batch_tiles(b, 16, 16);
+  int rc = batch_tiles(b, 24, 18);
   if (rc) { delete b; return rc; }
   *out = b;
   return PCOM_OK;
@@ -1029,11 +1120,15 @@ int pcom_gpu_batch_use_graphs(pcom_batch *b, int32_t enable) {
 
 int pcom_gpu_batch_den_prho(pcom_batch *b) {
   if (!b) return fail(PCOM_ERR_ARG, "null batch");
-  Dev *dP = nullptr;
-  int rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
+  int rc = batch_join_in(b);
   if (rc) return rc;
-  for (pcom_handle *h : b->hs) h->launches++;
+  Dev *dP = nullptr;
+  rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
+  if (rc) return rc;
+  b->launches++;
   launch_batch(BK_DEN_PRHO, dP, b->shape, 0, b->stream);
+  rc = batch_join_out(b);
+  if (rc) return rc;
   return batch_sync(b);
 }
 
@@ -1053,6 +1148,8 @@ int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
     h->D.ab3_mode = (fresh && tctr_i == 1) ? 1 : 0;
   }
   const bool startup = tctr_i <= 2;
+  int rc0 = batch_join_in(b);
+  if (rc0) return rc0;
   for (pcom_handle *h : b->hs)
     if (h->dims.rst != 1 && tctr_i == 2) {
       CK(cudaMemcpyAsync(h->D.aupp, h->D.aup, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, b->stream));
@@ -1083,9 +1180,11 @@ int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
     CK(cudaGraphLaunch(it->second, b->stream));
   }
   if (rc) return rc;
+  rc = batch_join_out(b);
+  if (rc) return rc;
+  b->launches += 12 + (int64_t)b->groups.size();  // kernels of one batched step
   for (pcom_handle *h : b->hs) {
     h->D.ab3_mode = 0;
-    h->launches += 14;
     h->n_ch++; h->n_uv++; h->n_ssh++; h->n_w++; h->n_ts++;
     // tc = tp = the buffer int_ts wrote (mod_int.f90:496-497)
     int fr = 0;
@@ -1095,6 +1194,17 @@ int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
   }
   return PCOM_OK;
 }
+
+int pcom_gpu_batch_set_tiles(pcom_batch *b, int32_t tx, int32_t ty, int32_t max_resident) {
+  if (!b) return fail(PCOM_ERR_ARG, "null batch");
+  if (tx < 1 || ty < 1 || (tx + 4) * (ty + 4) > 640)
+    return fail(PCOM_ERR_ARG, "tile %dx%d: need tx, ty >= 1 and (tx+4)*(ty+4) <= 640", tx, ty);
+  CK(cudaStreamSynchronize(b->stream));
+  b->max_resident = max_resident > 0 ? max_resident : 0;
+  return batch_tiles(b, tx, ty);
+}
+
+int64_t pcom_gpu_batch_launch_count(pcom_batch *b) { return b ? b->launches : 0; }
 
 int pcom_gpu_batch_sync(pcom_batch *b) {
   if (!b) return fail(PCOM_ERR_ARG, "null batch");
@@ -1107,22 +1217,47 @@ int pcom_gpu_batch_step(pcom_batch *b, int64_t tctr_i) {
   return batch_sync(b);
 }
 
-// Autotuner: time the batched barotropic kernel for candidate tile shapes on
-// the members' current state (the 2-D state it changes is saved and
-// restored around every trial) and keep the fastest.
+// Autotuner: time the barotropic launches of the whole batch for candidate
+// tile shapes on the members' current state (the 2-D fields they change are
+// saved and restored around every trial) and keep the fastest.  The choice
+// is cached per set of member grid sizes, so later batches of the same
+// shapes skip the trials.
 int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
   if (!b) return fail(PCOM_ERR_ARG, "null batch");
-  static const int cand[][2] = {{8, 8}, {16, 8}, {16, 16}, {24, 18}, {32, 8}, {32, 16}, {32, 24}, {48, 16}, {64, 8}};
+  static std::mutex cache_mu;
+  static std::map<std::string, std::pair<int, int>> cache;
+  std::vector<std::string> dims;
+  for (pcom_handle *h : b->hs) dims.push_back(std::to_string(h->dims.glo_ni) + "x" + std::to_string(h->dims.glo_nj));
+  std::sort(dims.begin(), dims.end());
+  std::string sig;
+  for (auto &d : dims) sig += d + ",";
+  {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    auto it = cache.find(sig);
+    if (it != cache.end()) {
+      int rc = batch_tiles(b, it->second.first, it->second.second);
+      if (rc) return rc;
+      std::string rep = "cached -> " + std::to_string(b->TX) + "x" + std::to_string(b->TY);
+      if (report && len > 0) { strncpy(report, rep.c_str(), (size_t)len - 1); report[len - 1] = 0; }
+      return PCOM_OK;
+    }
+  }
+  static const int cand[][2] = {{12, 12}, {16, 8},  {16, 12}, {16, 16}, {24, 12}, {20, 16},
+                                {24, 18}, {32, 8},  {32, 12}, {28, 16}, {48, 8},  {64, 6}};
+  for (cudaStream_t s : b->member_streams) CK(cudaStreamSynchronize(s));
+  CK(cudaStreamSynchronize(b->stream));
   // save the 2-D fields the subcycle writes
   std::vector<double *> saved;
   auto fields = [](pcom_handle *h) {
     return std::vector<double *>{h->D.chc, h->D.chp, h->D.mch, h->D.mch2, h->D.ubc, h->D.vbc, h->D.ubp, h->D.vbp, h->D.acch};
   };
+  int rc = 0;
   for (pcom_handle *h : b->hs)
     for (double *f : fields(h)) {
       double *c = nullptr;
-      CK(cudaMalloc(&c, h->n2 * sizeof(double)));
-      CK(cudaMemcpy(c, f, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice));
+      if (!rc && cudaMalloc(&c, h->n2 * sizeof(double)) != cudaSuccess) rc = fail(PCOM_ERR_CUDA, "autotune scratch");
+      if (!rc && cudaMemcpy(c, f, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess)
+        rc = fail(PCOM_ERR_CUDA, "autotune save");
       saved.push_back(c);
     }
   auto restore = [&]() -> int {
@@ -1132,7 +1267,7 @@ int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
     return PCOM_OK;
   };
   Dev *dP = nullptr;
-  int rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
+  if (!rc) rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
   double best = 1e30;
   int bx = b->TX, by = b->TY;
   std::string rep;
@@ -1141,13 +1276,13 @@ int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
   cudaEventCreate(&e1);
   for (auto &c : cand) {
     if (rc) break;
-    if (trop_batch_max_blocks(c[0], c[1]) <= 0) continue;
+    if (trop_group_max_blocks(c[0], c[1]) <= 0) continue;
     rc = batch_tiles(b, c[0], c[1]);
     if (rc) break;
     float ms = 0.f, tot = 0.f;
     for (int rep_i = 0; rep_i < 3 && !rc; ++rep_i) {
       cudaEventRecord(e0, b->stream);
-      cudaError_t e = launch_trop_batch(dP, b->dtiles, b->ntiles, b->TX, b->TY, b->nblocks, b->cnt, b->err, b->stream);
+      cudaError_t e = batch_trop(b, dP);
       cudaEventRecord(e1, b->stream);
       if (e != cudaSuccess) rc = fail(PCOM_ERR_CUDA, "autotune launch: %s", cudaGetErrorString(e));
       if (!rc) rc = batch_sync(b);
@@ -1156,8 +1291,11 @@ int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
       if (!rc) rc = restore();
     }
     const double t = tot / 2.0;
-    char line[96];
-    snprintf(line, sizeof line, "%dx%d:%.3fms(%d tiles,%d CTAs) ", c[0], c[1], t, b->ntiles, b->nblocks);
+    int res = 0, tiles = 0;
+    for (auto &g : b->groups) { res += g.resident; tiles += g.ntiles; }
+    char line[128];
+    snprintf(line, sizeof line, "%dx%d:%.3fms(%d tiles,%d launches,%d resident) ", c[0], c[1], t, tiles,
+             (int)b->groups.size(), res);
     rep += line;
     if (!rc && t < best) { best = t; bx = c[0]; by = c[1]; }
   }
@@ -1167,6 +1305,10 @@ int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
   if (rc) return rc;
   rc = batch_tiles(b, bx, by);
   if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    cache[sig] = {bx, by};
+  }
   char line[96];
   snprintf(line, sizeof line, "-> %dx%d", bx, by);
   rep += line;

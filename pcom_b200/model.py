@@ -222,6 +222,12 @@ class Batch:
         L.check(self.lib.pcom_gpu_batch_autotune(self._b, buf, 1024), "batch_autotune")
         return buf.value.decode()
 
+    def set_tiles(self, tx: int, ty: int, max_resident: int = 0):
+        L.check(self.lib.pcom_gpu_batch_set_tiles(self._b, tx, ty, max_resident), "batch_set_tiles")
+
+    def launch_count(self) -> int:
+        return int(self.lib.pcom_gpu_batch_launch_count(self._b))
+
     def close(self):
         if getattr(self, "_b", None) and self._b.value:
             self.lib.pcom_gpu_batch_destroy(self._b)

@@ -18,6 +18,9 @@ Cases
               0.1 sin(3 lat), SST/SSS restoring.
 ``global025`` 1440 x 640 x 30, the same generator at 0.25 deg with
               dtbt = 20 s, dtbc = 1200 s.
+``basin``     glo_ni x glo_nj x nk (default 64 x 32 x 20) flat-bottom 1 deg
+              basin centred on the equator, walls, box forcing; the uneven
+              basins of the batched-ensemble workload.
 ``tiny``, ``tiny_bathy``: small grids for fast parity tests.
 
 Vertical levels: z(k) = (k - 1/2) * 4000 m / nk, i.e. evenly spaced to about
@@ -70,7 +73,8 @@ def make_case(name: str = "box", seed: int = 1, noise: float = 0.01,
         lon = 2.0 * np.arange(ni_, dtype=np.float64) + 1.0
     elif name == "basin":
         ni_, nj_, nk_ = glo_ni or 64, glo_nj or 32, nk or 20
-        lat = -30.0 + 1.0 * np.arange(1, nj_ + 1, dtype=np.float64)
+        # 1 deg, centred on the equator (256 x 128 spans 63S-64N)
+        lat = -float(nj_ // 2) + np.arange(1, nj_ + 1, dtype=np.float64)
         lon = np.arange(ni_, dtype=np.float64) + 0.5
     elif name == "tiny_bathy":
         ni_, nj_, nk_ = 24, 14, 12

@@ -52,6 +52,34 @@ def test_batch_matches_sequential(graphs):
         m.close()
 
 
+def test_batch_packing_and_multitile_fallback():
+    """16x8 tiles with at most 40 tiles per co-resident group: the small
+    members are packed into groups (first-fit decreasing) and the box (72
+    tiles) falls back to the multi-tile kernel; results stay bit-equal."""
+    cases = _members() + [make_case("box")]
+    steps = 5
+    seq = []
+    for c in cases:
+        m = Model(c)
+        m.run(steps)
+        seq.append(m)
+    bm = [Model(c) for c in cases]
+    b = Batch(bm)
+    b.set_tiles(16, 8, max_resident=40)
+    b.run(steps)
+    for q, (x, y) in enumerate(zip(bm, seq)):
+        _assert_equal(x, y, f"member {q} ({cases[q]['name']}) with packed groups")
+    b.set_tiles(16, 8, max_resident=1)  # every member on the multi-tile kernel
+    b.run(2)
+    for m in seq:
+        m.run(2)
+    for q, (x, y) in enumerate(zip(bm, seq)):
+        _assert_equal(x, y, f"member {q} ({cases[q]['name']}) on the multi-tile kernel")
+    b.close()
+    for m in bm + seq:
+        m.close()
+
+
 def test_batch_autotune_keeps_results():
     cases = _members()[:3] + [make_case("box")]
     seq = []
@@ -67,6 +95,27 @@ def test_batch_autotune_keeps_results():
     b.run(2)
     for q, (x, y) in enumerate(zip(bm, seq)):
         _assert_equal(x, y, f"member {q} after autotune ({report})")
+    b.close()
+    for m in bm + seq:
+        m.close()
+
+
+def test_batch_on_caller_stream():
+    """Members on the caller's (legacy default) stream: the batch captures on
+    its own stream and joins the members' streams by events."""
+    cases = _members()[:2]
+    seq = []
+    for c in cases:
+        m = Model(c)
+        m.run(6)
+        seq.append(m)
+    bm = [Model(c) for c in cases]
+    for m in bm:
+        m.set_stream(0)
+    b = Batch(bm)
+    b.run(6)
+    for q, (x, y) in enumerate(zip(bm, seq)):
+        _assert_equal(x, y, f"member {q} on the default stream")
     b.close()
     for m in bm + seq:
         m.close()
