@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     p.add_argument("--workload", default="global1", choices=["global1", "ensemble"],
                    help="ensemble: 32 perturbed 1-degree members + 16 uneven basins, batched")
     p.add_argument("--members", type=int, default=32)
@@ -272,6 +273,13 @@ def run_ours(args):
     kernels = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(x[1] for x in prof.values())), 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
 
+    # ------------------------------------------------ mixed-precision path
+    # the same device-resident loop on a PCOM_PREC_MIXED handle, and the
+    # per-field error of a fresh pair of runs after one model day
+    mixed = None
+    if not args.no_mixed:
+        mixed = run_mixed_leg(args, case, stream, steps)
+
     # ------------------------------------------------ CPU baseline (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -310,12 +318,56 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "cpu_baseline": cpu,
+            "mixed": mixed,
         }
         print(json.dumps(line))
     m.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_mixed_leg(args, case, stream, steps):
+    import torch
+
+    from pcom_b200 import _lib as L
+    from pcom_b200.model import Model
+
+    mm = Model(case, flags=L.PCOM_PREC_MIXED)
+    mm.set_stream(stream.cuda_stream)
+    mm.run(max(args.warmup, 3))
+    it0 = mm.iter
+    day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for q in range(steps):
+        it = it0 + 1 + q
+        if day_of(it) != day_of(it - 1):
+            L.check(mm.lib.pcom_gpu_den_prho(mm.handle), "den_prho")
+        L.check(mm.lib.pcom_gpu_step_async(mm.handle, it), "step")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    mm.check_finite()
+    mm.close()
+    # error after one model day (24 steps) against the FP64 path
+    a, b = Model(case), Model(case, flags=L.PCOM_PREC_MIXED)
+    a.run(24)
+    b.run(24)
+    st = a.static()
+    k = np.arange(1, a.nk + 1)[:, None, None]
+    mk = {"t3": st["lev_t"][None] >= k, "u3": st["lev_u"][None] >= k, "t2": st["lev_t"] >= 1, "u2": st["lev_u"] >= 1}
+    which = {"tc": "t3", "sc": "t3", "uc": "u3", "vc": "u3", "chc": "t2", "ubc": "u2", "vbc": "u2"}
+    err = {}
+    for f, w in which.items():
+        x, y = b.field(f)[mk[w]], a.field(f)[mk[w]]
+        err[f] = float(np.sqrt(np.mean((x - y) ** 2)) / max(np.sqrt(np.mean(y * y)), 1e-30))
+    a.close()
+    b.close()
+    return {"ms_per_step": round(ms, 4), "value": round(sypd(ms / 1000.0), 2), "unit": "SYPD", "dtype": "f32 stencils, f64 barotropic",
+            "rel_rms_error_vs_fp64_after_24_steps": {k_: float(f"{v:.3e}") for k_, v in err.items()}}
 
 
 def ensemble_cases(members: int, basins: int, member_case: str = "box"):

@@ -38,7 +38,15 @@ extern "C" {
 
 /* pcom_dims.flags */
 #define PCOM_PREC_FP64 0x0   /* FP64 everywhere: the reference's arithmetic */
-#define PCOM_PREC_MIXED 0x1  /* FP32 stencils, FP64 bottom-pressure accumulation */
+/* Mixed: the 3-D fields are stored as FP32 and the advection, friction,
+ * diffusion, upwelling and Smagorinsky stencils compute in FP32; alpha and
+ * adp are stored as anomalies from a reference profile (fixed from the level
+ * means of the first T/S given to pcom_gpu_set_state); the barotropic
+ * subcycle and its ch/mch/mch2 accumulation, the pressure-gradient and AB3
+ * updates, the tracer update and the global sums stay FP64.  The ABI keeps
+ * FP64 host arrays: the library converts on upload and download.  No
+ * counterpart in the reference. */
+#define PCOM_PREC_MIXED 0x1
 #define PCOM_LIT_R8 0x10     /* default-REAL literals read as REAL(8) (ifort -r8);
                                 otherwise REAL(4) as gfortran compiles them */
 
@@ -147,6 +155,11 @@ int64_t pcom_gpu_field_size(pcom_handle *h, const char *name);
 /* Run the NaN/Inf watchdog over the prognostic fields; PCOM_ERR_NUMERIC if
  * any wet point is not finite. */
 int pcom_gpu_check_finite(pcom_handle *h);
+/* Global sums over the wet T cells of the interior: out3[0] = volume (m^3),
+ * out3[1] = sum of T dV (K m^3), out3[2] = sum of S dV (psu m^3), with
+ * dV = a^2 rh1 dx1x dx1y dz(k); FP64, in a fixed reduction order.  No
+ * counterpart in the reference. */
+int pcom_gpu_global_sums(pcom_handle *h, double *out3);
 
 /* --- streams and timing -------------------------------------------------- */
 /* Use an external CUDA stream (cudaStream_t as void*) for all work. */

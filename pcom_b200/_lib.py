@@ -101,6 +101,7 @@ SIGNATURES = {
     "pcom_gpu_launch_count": (C.c_int64, [C.c_void_p]),
     "pcom_gpu_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
     "pcom_gpu_trop_noalloc": (C.c_int, [C.POINTER(TropIO), C.c_void_p]),
+    "pcom_gpu_global_sums": (C.c_int, [C.c_void_p, dbl_p]),
     "pcom_gpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
     "pcom_gpu_batch_destroy": (C.c_int, [C.c_void_p]),
     "pcom_gpu_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),

@@ -14,6 +14,8 @@
 // division by a static metric, a bottom pressure or a per-step 2-D field uses
 // its precomputed correctly rounded reciprocal with dvr (bitwise equal to the
 // IEEE quotient); the equation of state keeps its IEEE divisions.
+#include <type_traits>
+
 #include "pcom_dev.cuh"
 #include "pcom_kernels.h"
 
@@ -39,7 +41,8 @@ namespace {
 #define DIVDP(x, k) dvr((x), P.dpr2[k], P.rdpr2[k])
 
 // column/row of this thread; interior: i in 2..ni-1, else i in 1..ni
-__device__ __forceinline__ bool cell(const Dev &P, int &i, int &j, bool interior) {
+template <typename R>
+__device__ __forceinline__ bool cell(const DevT<R> &P, int &i, int &j, bool interior) {
   const int x = blockIdx.x * TB_X + threadIdx.x;
   j = blockIdx.y + 1;
   if (interior) {
@@ -53,9 +56,11 @@ __device__ __forceinline__ bool cell(const Dev &P, int &i, int &j, bool interior
 // ----------------------------------------------------------------------------
 // den_alpha (mod_den.f90:33-55) with T, S = tc, sc and ch = chc, fused with
 // int_tobot (mod_op.f90:927-944) -> adp.
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   double *tmp = sh;  // [nk][TB_X]
   int i, j;
@@ -71,9 +76,9 @@ __global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev
     double al;
     if (k <= lev) {
       al = 1.0 / den_rho(P.c, P.tc[q], P.sc[q], ch * P.pr2[k]);
-      P.alpha[q] = al;
+      P.alpha[q] = alpha_store(P, al, k);
     } else {
-      al = P.alpha[q];
+      al = alpha_full(P, P.alpha[q], k);
     }
     tmp[(k - 1) * TB_X + tx] = al * P.dpr2[k] * (double)(k <= lev);
   }
@@ -88,7 +93,7 @@ __global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev
     } else {
       v = tmp[(nk - 1) * TB_X + tx] * 0.5;
     }
-    P.adp[q2 + P.n2 * (k - 1)] = v;
+    P.adp[q2 + P.n2 * (k - 1)] = adp_store(P, v, k, q2);
   }
 }
 
@@ -96,9 +101,11 @@ __global__ void __launch_bounds__(512) k_alpha_tobot(const __grid_constant__ Dev
 // int_pgra (mod_int.f90:64-88): bphi and bgraphi, the column integrals of the
 // E/N-averaged geopotential and of the adp gradient (op_vint_ns/op_vint_ew,
 // mod_op.f90:946-981, incl. their cshift(-1) masks).
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *bE = sh, *bN = sh + nk * TB_X, *bX = sh + 2 * nk * TB_X, *bY = sh + 3 * nk * TB_X;
@@ -111,12 +118,12 @@ __global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P0, 
     if (!ok) continue;
     const long long q = q2 + P.n2 * (k - 1);
     const double dp = P.dpr2[k], pr = P.pr2[k];
-    const double adc = ld(P.adp, q), ade = ld(P.adp, q + 1);
-    const double alc = ld(P.alpha, q), ale = ld(P.alpha, q + 1);
+    const double adc = adp_full(P, ld(P.adp, q), k, q2), ade = adp_full(P, ld(P.adp, q + 1), k, q2 + 1);
+    const double alc = alpha_full(P, ld(P.alpha, q), k), ale = alpha_full(P, ld(P.alpha, q + 1), k);
     const double wkE = 0.5 * (adc + ade) + pr * (0.5 * (alc + ale));
     double wkN = 0.0, wky = 0.0;
     if (nrow) {
-      const double adn = ld(P.adp, q + P.ni), aln = ld(P.alpha, q + P.ni);
+      const double adn = adp_full(P, ld(P.adp, q + P.ni), k, q2 + P.ni), aln = alpha_full(P, ld(P.alpha, q + P.ni), k);
       wkN = 0.5 * (adc + adn) + pr * (0.5 * (alc + aln));
       wky = DIVA(DIVY(adn - adc, 4, j));
     }
@@ -153,9 +160,11 @@ __global__ void __launch_bounds__(512) k_pgra2d(const __grid_constant__ Dev P0, 
 //     1/mch, 1/(g mch2)
 //  mode 2 (int_clin, mod_int.f90:318-320, 385-386): sqrt(ter(mch, dft 1))
 //     with 1 on land, sqrt(ter(mch2, dft 1)), 1/mch2
-template <bool BATCH>
-__global__ void k_uv2d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, int mode) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void k_uv2d(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps, int mode) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   if (x >= P.glo_ni || j > P.nj) return;
@@ -198,9 +207,11 @@ __global__ void k_uv2d(const __grid_constant__ Dev P0, const Dev *__restrict__ P
 // upwelling (mod_int.f90:626-647): wk3d = div(sqrt(ter(chp)) * (uc, vc)),
 // wm(k) = (wm(k-1) + dpr(k-1) (wk3d(k-1) - vint(wk3d))) msk(k).
 // with_acw: also int_ts's acw accumulation (mod_int.f90:458-461).
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, int with_acw) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps, int with_acw) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *wk = sh, *tm = sh + nk * TB_X, *wmv = sh + 2 * nk * TB_X;
@@ -214,23 +225,23 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P
   for (int k = threadIdx.y + 1; k <= nk; k += TB_K) {
     if (!ok) continue;
     const long long o = P.n2 * (k - 1);
-    const double s_c = ld(P.sch_w, q2), s_w = ld(P.sch_w, qw);
-    const double r_c = RH(3, j);
+    const R s_c = ld(P.sch_w, q2), s_w = ld(P.sch_w, qw);
+    const R r_c = RH(3, j);
     // p1(ter_{U->E}(sch uc)): tE(i') = 0.5 (va(i', j-1) + va(i', j)) for j >= 2
-    double tEc = 0.0, tEw = 0.0, B = 0.0;
+    R tEc = 0.0, tEw = 0.0, B = 0.0;
     if (srow) {
-      const double s_s = ld(P.sch_w, qs), s_sw = ld(P.sch_w, qsw), r_s = RH(3, j - 1);
+      const R s_s = ld(P.sch_w, qs), s_sw = ld(P.sch_w, qsw), r_s = RH(3, j - 1);
       tEc = 0.5 * (s_s * ld(P.uc, qs + o) + s_c * ld(P.uc, q2 + o));
       tEw = 0.5 * (s_sw * ld(P.uc, qsw + o) + s_w * ld(P.uc, qw + o));
       // p2(ter_{U->N}(sch vc rh3)): tN(j') = 0.5 (x(i-1, j') + x(i, j'))
-      const double tNc = 0.5 * (s_w * ld(P.vc, qw + o) * r_c + s_c * ld(P.vc, q2 + o) * r_c);
-      const double tNs = 0.5 * (s_sw * ld(P.vc, qsw + o) * r_s + s_s * ld(P.vc, qs + o) * r_s);
+      const R tNc = 0.5 * (s_w * ld(P.vc, qw + o) * r_c + s_c * ld(P.vc, q2 + o) * r_c);
+      const R tNs = 0.5 * (s_sw * ld(P.vc, qsw + o) * r_s + s_s * ld(P.vc, qs + o) * r_s);
       B = DIVY(tNc - tNs, 1, j);
     }
-    const double A = DIVX(tEc - tEw, 1, i);
-    const double w = DIVARH(A + B, 1, j);
+    const R A = DIVX(tEc - tEw, 1, i);
+    const R w = DIVARH(A + B, 1, j);
     wk[(k - 1) * TB_X + tx] = w;
-    tm[(k - 1) * TB_X + tx] = w * P.dpr2[k] * (double)(k <= lev);
+    tm[(k - 1) * TB_X + tx] = w * P.dpr2[k] * (R)(k <= lev);
   }
   __syncthreads();
   if (ok && threadIdx.y == 0) {
@@ -254,7 +265,7 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P
     if (k >= 2) st2(P.wm, P, i, q, w);
     if (with_acw) {
       const double gm = P.c.g * ld(P.mch2, q2);
-      st2(P.acw, P, i, q, P.acw[q] + dvr(w * ld(P.alpha, q), gm, ld(P.rgm2, q2)));
+      st2(P.acw, P, i, q, P.acw[q] + dvr(w * alpha_full(P, ld(P.alpha, q), k), gm, ld(P.rgm2, q2)));
     }
   }
 }
@@ -263,9 +274,11 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ Dev P
 // int_readyc 3-D part (mod_int.f90:114-149): op_adv for uc and vc
 // (mod_op.f90:224-278), op_fri -> fri_r3d for both components
 // (mod_op.f90:103-184) and the depth integral of the baroclinic tendency.
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *tu = sh, *tv = sh + nk * TB_X;
@@ -274,49 +287,49 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0
   const int tx = threadIdx.x;
   const long long q2 = ok ? I2(P, i, j) : 0;
   const int ni = P.ni;
-  const double g = P.c.g, a = P.c.a;
-  const double grho = g * P.c.rho0;
+  const R g = P.c.g, a = P.c.a;
+  const R grho = g * P.c.rho0;
   const bool nrow = j <= P.njm, srow = j >= 2;
   const long long qe = q2 + 1, qw = q2 - 1, qn = q2 + ni, qs = q2 - ni;
   const int lu = ok ? P.lev_u[q2] : 0;
   for (int k = threadIdx.y + 1; k <= nk && ok; k += TB_K) {
     const long long o = P.n2 * (k - 1);
     // per-column coefficients
-    const double sch = ld(P.sch_r, q2), rsch = ld(P.rsch, q2);
-    const double rsc_e = ld(P.rsch, qe), rsc_w = ld(P.rsch, qw);
-    const double sch_e = ld(P.sch_r, qe), sch_w = ld(P.sch_r, qw);
-    const double rh3 = RH(3, j), dx3 = MX(3, i), rdx3 = RMX(3, i), dy3 = MY(3, j), rdy3 = RMY(3, j);
-    const double arh3 = ARH(3, j), rarh3 = RARH(3, j);
-    const double mu_k = (double)(lu >= k), mu_k1 = (double)(lu >= k + 1), mu_km = (double)(lu >= k - 1);
+    const R sch = ld(P.sch_r, q2), rsch = ld(P.rsch, q2);
+    const R rsc_e = ld(P.rsch, qe), rsc_w = ld(P.rsch, qw);
+    const R sch_e = ld(P.sch_r, qe), sch_w = ld(P.sch_r, qw);
+    const R rh3 = RH(3, j), dx3 = MX(3, i), rdx3 = RMX(3, i), dy3 = MY(3, j), rdy3 = RMY(3, j);
+    const R arh3 = ARH(3, j), rarh3 = RARH(3, j);
+    const R mu_k = (R)(lu >= k), mu_k1 = (R)(lu >= k + 1), mu_km = (R)(lu >= k - 1);
     auto U = [&](long long q, int kk) { return ld(P.uc, q + P.n2 * (kk - 1)); };
     auto V = [&](long long q, int kk) { return ld(P.vc, q + P.n2 * (kk - 1)); };
     // velocities at level k (unweighted wu = uc/sch, wv = vc/sch)
-    const double u_c = U(q2, k), u_e = U(qe, k), u_w = U(qw, k);
-    const double v_c = V(q2, k), v_e = V(qe, k), v_w = V(qw, k);
-    const double wu_c = dvr(u_c, sch, rsch), wu_e = dvr(u_e, sch_e, rsc_e), wu_w = dvr(u_w, sch_w, rsc_w);
-    const double wv_c = dvr(v_c, sch, rsch), wv_e = dvr(v_e, sch_e, rsc_e), wv_w = dvr(v_w, sch_w, rsc_w);
-    double u_n = 0, u_s = 0, v_n = 0, v_s = 0, wu_n = 0, wu_s = 0, wv_n = 0, wv_s = 0, rh3n = 0, rh3s = 0;
+    const R u_c = U(q2, k), u_e = U(qe, k), u_w = U(qw, k);
+    const R v_c = V(q2, k), v_e = V(qe, k), v_w = V(qw, k);
+    const R wu_c = dvr(u_c, sch, rsch), wu_e = dvr(u_e, sch_e, rsc_e), wu_w = dvr(u_w, sch_w, rsc_w);
+    const R wv_c = dvr(v_c, sch, rsch), wv_e = dvr(v_e, sch_e, rsc_e), wv_w = dvr(v_w, sch_w, rsc_w);
+    R u_n = 0, u_s = 0, v_n = 0, v_s = 0, wu_n = 0, wu_s = 0, wv_n = 0, wv_s = 0, rh3n = 0, rh3s = 0;
     if (nrow) {
-      const double sn = ld(P.sch_r, qn), rsn = ld(P.rsch, qn);
+      const R sn = ld(P.sch_r, qn), rsn = ld(P.rsch, qn);
       u_n = U(qn, k); v_n = V(qn, k);
       wu_n = dvr(u_n, sn, rsn); wv_n = dvr(v_n, sn, rsn);
       rh3n = RH(3, j + 1);
     }
     if (srow) {
-      const double ss = ld(P.sch_r, qs), rss = ld(P.rsch, qs);
+      const R ss = ld(P.sch_r, qs), rss = ld(P.rsch, qs);
       u_s = U(qs, k); v_s = V(qs, k);
       wu_s = dvr(u_s, ss, rss); wv_s = dvr(v_s, ss, rss);
       rh3s = RH(3, j - 1);
     }
     // vertical neighbours at (i, j)
-    const double u_km = (k > 1) ? U(q2, k - 1) : 0.0, v_km = (k > 1) ? V(q2, k - 1) : 0.0;
-    const double u_k1 = (k < nk) ? U(q2, k + 1) : 0.0, v_k1 = (k < nk) ? V(q2, k + 1) : 0.0;
+    const R u_km = (k > 1) ? U(q2, k - 1) : 0.0, v_km = (k > 1) ? V(q2, k - 1) : 0.0;
+    const R u_k1 = (k < nk) ? U(q2, k + 1) : 0.0, v_k1 = (k < nk) ? V(q2, k + 1) : 0.0;
     // u on N (i, j), (i+1, j); v*cos on E (i, j), (i, j+1)
-    const double uN0 = 0.5 * (wu_w + wu_c), uN1 = 0.5 * (wu_c + wu_e);
-    const double vE0 = srow ? 0.5 * (wv_s * rh3s + wv_c * rh3) : 0.0;
-    const double vE1 = nrow ? 0.5 * (wv_c * rh3 + wv_n * rh3n) : 0.0;
+    const R uN0 = 0.5 * (wu_w + wu_c), uN1 = 0.5 * (wu_c + wu_e);
+    const R vE0 = srow ? 0.5 * (wv_s * rh3s + wv_c * rh3) : 0.0;
+    const R vE1 = nrow ? 0.5 * (wv_c * rh3 + wv_n * rh3n) : 0.0;
     // w on U: ter_{T->U}(wm / chc) (di, rows j <= njm)
-    auto wU = [&](int kk) -> double {
+    auto wU = [&](int kk) -> R {
       if (!nrow) return 0.0;
       const long long ok_ = P.n2 * (kk - 1);
       const long long t00 = q2, t01 = qn, t10 = qe, t11 = qn + 1;
@@ -325,80 +338,80 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0
               dvr(ld(P.wm, t10 + ok_), ld(P.chc, t10), ld(P.rchc, t10)) +
               dvr(ld(P.wm, t11 + ok_), ld(P.chc, t11), ld(P.rchc, t11))) * 0.25;
     };
-    const double wUk = wU(k), wUk1 = wU(k + 1);
-    const double dm1 = dvr(uN1 - uN0, dx3, rdx3);
-    const double dm2 = nrow ? dvr(vE1 - vE0, dy3, rdy3) : 0.0;
-    const double dw = DIVDP(wUk - wUk1, k);
-    const double rdiv = dvr(dm1 + dm2, arh3, rarh3) + dw;
+    const R wUk = wU(k), wUk1 = wU(k + 1);
+    const R dm1 = dvr(uN1 - uN0, dx3, rdx3);
+    const R dm2 = nrow ? dvr(vE1 - vE0, dy3, rdy3) : 0.0;
+    const R dw = DIVDP(wUk - wUk1, k);
+    const R rdiv = dvr(dm1 + dm2, arh3, rarh3) + dw;
     // op_adv(var)
-    auto adv = [&](double x_c, double x_e, double x_w, double x_n, double x_s, double x_km, double x_k1) {
-      const double wk1_0 = (0.5 * (x_w + x_c)) * uN0, wk1_1 = (0.5 * (x_c + x_e)) * uN1;
-      const double wk2_0 = srow ? (0.5 * (x_s + x_c)) * vE0 : 0.0;
-      const double wk2_1 = nrow ? (0.5 * (x_c + x_n)) * vE1 : 0.0;
-      const double wa = dvr(wk1_1 - wk1_0, dx3, rdx3);
-      const double wb = nrow ? dvr(wk2_1 - wk2_0, dy3, rdy3) : 0.0;
-      double ans = dvr(wa + wb, arh3, rarh3);
+    auto adv = [&](R x_c, R x_e, R x_w, R x_n, R x_s, R x_km, R x_k1) {
+      const R wk1_0 = (0.5 * (x_w + x_c)) * uN0, wk1_1 = (0.5 * (x_c + x_e)) * uN1;
+      const R wk2_0 = srow ? (0.5 * (x_s + x_c)) * vE0 : 0.0;
+      const R wk2_1 = nrow ? (0.5 * (x_c + x_n)) * vE1 : 0.0;
+      const R wa = dvr(wk1_1 - wk1_0, dx3, rdx3);
+      const R wb = nrow ? dvr(wk2_1 - wk2_0, dy3, rdy3) : 0.0;
+      R ans = dvr(wa + wb, arh3, rarh3);
       // wkbp(kk) = vter(var)(kk) w(kk) msk(kk-1) msk(kk) for 2 <= kk <= nk
-      const double wkbp_k = (k >= 2) ? ((x_km + x_c) * 0.5 * wUk) * mu_km * mu_k : 0.0;
-      const double wkbp_k1 = (k < nk) ? ((x_c + x_k1) * 0.5 * wUk1) * mu_k * mu_k1 : 0.0;
+      const R wkbp_k = (k >= 2) ? ((x_km + x_c) * 0.5 * wUk) * mu_km * mu_k : 0.0;
+      const R wkbp_k1 = (k < nk) ? ((x_c + x_k1) * 0.5 * wUk1) * mu_k * mu_k1 : 0.0;
       ans = ans + DIVDP(wkbp_k - wkbp_k1, k);
       ans = ans - 0.5 * x_c * rdiv;
       return ans * mu_k;
     };
-    const double auc = adv(u_c, u_e, u_w, u_n, u_s, u_km, u_k1);
-    const double avc = adv(v_c, v_e, v_w, v_n, v_s, v_km, v_k1);
+    const R auc = adv(u_c, u_e, u_w, u_n, u_s, u_km, u_k1);
+    const R avc = adv(v_c, v_e, v_w, v_n, v_s, v_km, v_k1);
     // fri_r3d(ans, sch, v, vp, vc, tau)
-    const double am = ld(P.am, q2 + o);
-    const double cv1 = ld(P.cv1, q2), cv2 = ld(P.cv2, q2);
-    const double dx4 = MX(4, i), dx4e = MX(4, i + 1);
-    const double c00 = ld(P.chc, q2), c10 = ld(P.chc, qe);
-    const double c01 = nrow ? ld(P.chc, qn) : 0.0, c11 = nrow ? ld(P.chc, qn + 1) : 0.0;
-    const double chN0 = nrow ? 0.5 * (c00 + c01) : 0.0, chN1 = nrow ? 0.5 * (c10 + c11) : 0.0;
-    const double chE0 = 0.5 * (c00 + c10), chE1 = nrow ? 0.5 * (c01 + c11) : 0.0;
-    const double rh2 = RH(2, j), rh2n = nrow ? RH(2, j + 1) : 0.0;
-    const double dxc = a * RH(4, j) * (dx4 + dx4e);
-    const double rdxc = 1.0 / dxc;
+    const R am = ld(P.am, q2 + o);
+    const R cv1 = ld(P.cv1, q2), cv2 = ld(P.cv2, q2);
+    const R dx4 = MX(4, i), dx4e = MX(4, i + 1);
+    const R c00 = ld(P.chc, q2), c10 = ld(P.chc, qe);
+    const R c01 = nrow ? ld(P.chc, qn) : 0.0, c11 = nrow ? ld(P.chc, qn + 1) : 0.0;
+    const R chN0 = nrow ? 0.5 * (c00 + c01) : 0.0, chN1 = nrow ? 0.5 * (c10 + c11) : 0.0;
+    const R chE0 = 0.5 * (c00 + c10), chE1 = nrow ? 0.5 * (c01 + c11) : 0.0;
+    const R rh2 = RH(2, j), rh2n = nrow ? RH(2, j + 1) : 0.0;
+    const R dxc = a * RH(4, j) * (dx4 + dx4e);
+    const R rdxc = 1.0 / dxc;
     const int lev1 = lu;
-    auto fri = [&](double vc_, double ve_, double vw_, double vn_, double vs_, double vp_km, double vp_c,
-                   double vp_k1, double vce, double vcw, double v_bot_k, double vc_bot_k, double v_bot_km,
-                   double vc_bot_km, double tau) -> double {
-      const double wx0 = DIVARH(dvr(vc_ - vw_, dx4, RMX(4, i)), 4, j);
-      const double wx1 = DIVARH(dvr(ve_ - vc_, dx4e, RMX(4, i + 1)), 4, j);
-      const double wy0 = srow ? DIVA(DIVY(vc_ - vs_, 2, j)) : 0.0;
-      const double wy1 = nrow ? DIVA(DIVY(vn_ - vc_, 2, j + 1)) : 0.0;
-      const double va0 = chN0 * wx0, va1 = chN1 * wx1;
-      const double vb0 = (chE0 * wy0) * rh2, vb1 = (chE1 * wy1) * rh2n;
-      const double A = dvr(va1 - va0, dx3, rdx3);
-      const double B = nrow ? dvr(vb1 - vb0, dy3, rdy3) : 0.0;
-      const double wka = dvr(A + B, arh3, rarh3);
-      double ans = dvr(am, sch, rsch) * wka;
+    auto fri = [&](R vc_, R ve_, R vw_, R vn_, R vs_, R vp_km, R vp_c,
+                   R vp_k1, R vce, R vcw, R v_bot_k, R vc_bot_k, R v_bot_km,
+                   R vc_bot_km, R tau) -> R {
+      const R wx0 = DIVARH(dvr(vc_ - vw_, dx4, RMX(4, i)), 4, j);
+      const R wx1 = DIVARH(dvr(ve_ - vc_, dx4e, RMX(4, i + 1)), 4, j);
+      const R wy0 = srow ? DIVA(DIVY(vc_ - vs_, 2, j)) : 0.0;
+      const R wy1 = nrow ? DIVA(DIVY(vn_ - vc_, 2, j + 1)) : 0.0;
+      const R va0 = chN0 * wx0, va1 = chN1 * wx1;
+      const R vb0 = (chE0 * wy0) * rh2, vb1 = (chE1 * wy1) * rh2n;
+      const R A = dvr(va1 - va0, dx3, rdx3);
+      const R B = nrow ? dvr(vb1 - vb0, dy3, rdy3) : 0.0;
+      const R wka = dvr(A + B, arh3, rarh3);
+      R ans = dvr(am, sch, rsch) * wka;
       ans = ans + am * cv1 * vp_c;
-      const double pxc = dvr(vce - vcw, dxc, rdxc);
+      const R pxc = dvr(vce - vcw, dxc, rdxc);
       ans = ans + am * cv2 * sch * pxc;
       // wkp at kk = k and k+1: surface stress, bottom drag at lev+1, else
       // the km-scaled pz (mod_op.f90:147-161)
-      auto wkp = [&](int kk, double vp_a, double vp_b, double v_bot, double vc_bot) -> double {
+      auto wkp = [&](int kk, R vp_a, R vp_b, R v_bot, R vc_bot) -> R {
         if (kk == 1) return dvr(g * tau, sch, rsch);
         if (lev1 > 0 && kk == lev1 + 1) {
-          const double mag = sqrt(v_bot * v_bot + vc_bot * vc_bot);
+          const R mag = sqrt(v_bot * v_bot + vc_bot * vc_bot);
           return dvr(v_bot * g * P.c.cdbot * mag, sch, rsch);
         }
         if (kk > nk) return 0.0;
-        const double pzv = dvr((vp_a - vp_b) * (double)(lev1 >= kk - 1) * (double)(lev1 >= kk), P.dz1[kk], P.rdz1[kk]);
+        const R pzv = dvr((vp_a - vp_b) * (R)(lev1 >= kk - 1) * (R)(lev1 >= kk), P.dz1[kk], P.rdz1[kk]);
         return dvr(grho * ld(P.km, q2 + P.n2 * (kk - 1)) * pzv, sch * sch, ld(P.rsch2, q2));
       };
-      const double wkp_k = wkp(k, vp_km, vp_c, v_bot_km, vc_bot_km);
-      const double wkp_k1 = wkp(k + 1, vp_c, vp_k1, v_bot_k, vc_bot_k);
+      const R wkp_k = wkp(k, vp_km, vp_c, v_bot_km, vc_bot_km);
+      const R wkp_k1 = wkp(k + 1, vp_c, vp_k1, v_bot_k, vc_bot_k);
       return ans * mu_k + DIVDP(wkp_k - wkp_k1, k);
     };
     // level k-1 values for a bottom drag at kk = k (lev = k-1)
-    double wu_km = 0.0, wv_km = 0.0;
+    R wu_km = 0.0, wv_km = 0.0;
     if (k > 1 && lev1 == k - 1) { wu_km = dvr(u_km, sch, rsch); wv_km = dvr(v_km, sch, rsch); }
-    const double tx_ = ld(P.taux, q2), ty_ = ld(P.tauy, q2);
+    const R tx_ = ld(P.taux, q2), ty_ = ld(P.tauy, q2);
     // fx = fri(v = uc/sch, vp = uc, vc = -(vc/sch), taux)
-    const double fx = fri(wu_c, wu_e, wu_w, wu_n, wu_s, u_km, u_c, u_k1, -wv_e, -wv_w, wu_c, -wv_c, wu_km, -wv_km, tx_);
+    const R fx = fri(wu_c, wu_e, wu_w, wu_n, wu_s, u_km, u_c, u_k1, -wv_e, -wv_w, wu_c, -wv_c, wu_km, -wv_km, tx_);
     // fy = fri(v = vc/sch, vp = vc, vc = uc/sch, tauy)
-    const double fy = fri(wv_c, wv_e, wv_w, wv_n, wv_s, v_km, v_c, v_k1, wu_e, wu_w, wv_c, wu_c, wv_km, wu_km, ty_);
+    const R fy = fri(wv_c, wv_e, wv_w, wv_n, wv_s, v_km, v_c, v_k1, wu_e, wu_w, wv_c, wu_c, wv_km, wu_km, ty_);
     const long long q = q2 + o;
     st2(P.auc, P, i, q, auc);
     st2(P.avc, P, i, q, avc);
@@ -408,11 +421,11 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0
     }
     st2(P.fx, P, i, q, fx);
     st2(P.fy, P, i, q, fy);
-    const double pax = ld(P.pax, q2), pay = ld(P.pay, q2);
-    const double wx = -auc - sch * P.c.a0 * pax + fx;
-    const double wy = -avc - sch * P.c.a0 * pay + fy;
-    tu[(k - 1) * TB_X + tx] = wx * P.dpr2[k] * mu_k;
-    tv[(k - 1) * TB_X + tx] = wy * P.dpr2[k] * mu_k;
+    const R pax = ld(P.pax, q2), pay = ld(P.pay, q2);
+    const R wx = -auc - sch * P.c.a0 * pax + fx;
+    const R wy = -avc - sch * P.c.a0 * pay + fy;
+    tu[(k - 1) * TB_X + tx] = (double)wx * P.dpr2[k] * (double)mu_k;
+    tv[(k - 1) * TB_X + tx] = (double)wy * P.dpr2[k] * (double)mu_k;
   }
   __syncthreads();
   if (!ok || threadIdx.y >= 2) return;
@@ -425,9 +438,11 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ Dev P0
 // ----------------------------------------------------------------------------
 // int_clin (mod_int.f90:298-396): baroclinic momentum, barotropic
 // replacement, unweighted velocity and its accumulation.  smag runs after.
-template <bool BATCH>
-__global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *t1s = sh, *t2s = sh + nk * TB_X, *wsum = sh + 2 * nk * TB_X;
@@ -451,8 +466,8 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P0,
     const long long o = P.n2 * (k - 1);
     const double ph00 = ld(P.phih_t, q2), ph10 = ld(P.phih_t, qe);
     const double m00 = ld(P.mch, q2), m10 = ld(P.mch, qe);
-    const double ad00 = ld(P.adp, q2 + o), ad10 = ld(P.adp, qe + o);
-    const double al00 = ld(P.alpha, q2 + o), al10 = ld(P.alpha, qe + o);
+    const double ad00 = adp_full(P, ld(P.adp, q2 + o), k, q2), ad10 = adp_full(P, ld(P.adp, qe + o), k, qe);
+    const double al00 = alpha_full(P, ld(P.alpha, q2 + o), k), al10 = alpha_full(P, ld(P.alpha, qe + o), k);
     const double wk00 = ph00 + m00 * ad00, wk10 = ph10 + m10 * ad10;
     // px on E (i, j) and (i, j+1): gra(phih + mch adp) + ter(alpha) pr gra(mch)
     const double px0 = DIVARH(DIVX(wk10 - wk00, 2, i), 2, j) + 0.5 * (al00 + al10) * pr * mx0;
@@ -460,8 +475,8 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P0,
     if (nrow) {
       const double ph01 = ld(P.phih_t, qn), ph11 = ld(P.phih_t, qn + 1);
       const double m01 = ld(P.mch, qn), m11 = ld(P.mch, qn + 1);
-      const double ad01 = ld(P.adp, qn + o), ad11 = ld(P.adp, qn + 1 + o);
-      const double al01 = ld(P.alpha, qn + o), al11 = ld(P.alpha, qn + 1 + o);
+      const double ad01 = adp_full(P, ld(P.adp, qn + o), k, qn), ad11 = adp_full(P, ld(P.adp, qn + 1 + o), k, qn + 1);
+      const double al01 = alpha_full(P, ld(P.alpha, qn + o), k), al11 = alpha_full(P, ld(P.alpha, qn + 1 + o), k);
       const double wk01 = ph01 + m01 * ad01, wk11 = ph11 + m11 * ad11;
       const double px1 = DIVARH(DIVX(wk11 - wk01, 2, i), 2, j + 1) + 0.5 * (al01 + al11) * pr * mx1;
       t1 = 0.5 * (px0 + px1);
@@ -533,38 +548,43 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ Dev P0,
 
 // ----------------------------------------------------------------------------
 // smag (mod_int.f90:403-440): Smagorinsky viscosity, rows 2..nj-1.
-template <bool BATCH>
-__global__ void k_smag(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void k_smag(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
   if (x >= P.glo_ni || j > P.nj - 1) return;
   const int i = x + 2;
   const long long q2 = I2(P, i, j);
   const int ni = P.ni;
-  const double dx = ld(P.dxs, q2), rdx = ld(P.rdxs, q2);
-  const double dy = __ldg(P.dys1d + j - 1), rdy = __ldg(P.rdys1d + j - 1);
-  const double tn = ld(P.tn3, q2);
-  const double *u = P.uu, *v = P.vv;
+  const R dx = ld(P.dxs, q2), rdx = ld(P.rdxs, q2);
+  const R dy = __ldg(P.dys1d + j - 1), rdy = __ldg(P.rdys1d + j - 1);
+  const R tn = ld(P.tn3, q2);
+  const R *u = P.uu, *v = P.vv;
   for (int k = 1; k <= P.nk; ++k) {
   const long long q = q2 + P.n2 * (k - 1);
-  const double dt = dvr(4 * (ld(u, q + 1) - ld(u, q - 1)), dx, rdx) - dvr(4 * (ld(v, q + ni) - ld(v, q - ni)), dy, rdy) +
+  const R dt = dvr(4 * (ld(u, q + 1) - ld(u, q - 1)), dx, rdx) - dvr(4 * (ld(v, q + ni) - ld(v, q - ni)), dy, rdy) +
                     DIVA(ld(v, q) * tn);
-  const double ds = dvr(4 * (ld(v, q + 1) - ld(v, q - 1)), dx, rdx) + dvr(4 * (ld(u, q + ni) - ld(u, q - ni)), dy, rdy) -
+  const R ds = dvr(4 * (ld(v, q + 1) - ld(v, q - 1)), dx, rdx) + dvr(4 * (ld(u, q + ni) - ld(u, q - ni)), dy, rdy) -
                     DIVA(ld(u, q) * tn);
-  double c = 0.5 * P.c.smag_c / P.c.pi * (0.5 * dx + 0.5 * dy);
+  R c = 0.5 * P.c.smag_c / P.c.pi * (0.5 * dx + 0.5 * dy);
   c = c * c;
-  const double wk = c * sqrt(dt * dt + ds * ds);
-  const double am_max = dvr(dx * dx + dy * dy, (double)(4 * 8 * P.bc), P.rbc32);
+  const R wk = c * sqrt(dt * dt + ds * ds);
+  const R am_max = dvr(dx * dx + dy * dy, (R)(4 * 8 * P.bc), P.rbc32);
   st2(P.am, P, i, q, wk < am_max ? wk : am_max);
+  if (MIXED && k == 1) st2(P.am1, P, i, q, wk < am_max ? wk : am_max);
   }
 }
 
 // ----------------------------------------------------------------------------
 // int_ssh (mod_int.f90:602-624): alpha from (tp, sp, mch), SSH accumulation.
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   int i, j;
@@ -578,9 +598,9 @@ __global__ void __launch_bounds__(512) k_ssh(const __grid_constant__ Dev P0, con
     double al;
     if (k <= lev) {
       al = 1.0 / den_rho(P.c, P.tp[q], P.sp[q], mch * P.pr2[k]);
-      P.alpha[q] = al;
+      P.alpha[q] = alpha_store(P, al, k);
     } else {
-      al = P.alpha[q];
+      al = alpha_full(P, P.alpha[q], k);
     }
     sh[(k - 1) * TB_X + tx] = al * P.dpr2[k] * mch * (double)(k <= lev);
   }
@@ -606,7 +626,8 @@ struct Col {  // one column of T, S and prho in shared memory, stride TB_X
   __device__ double P2(int k) const { return p2[(k - 1) * TB_X]; }
 };
 
-__device__ void ts_mix(const Dev &P, long long q2, Col &c, double *rhoa, double *rhob, int na, int nb) {
+template <typename R>
+__device__ void ts_mix(const DevT<R> &P, long long q2, Col &c, double *rhoa, double *rhob, int na, int nb) {
   double st = 0.0, sd = 0.0;
   for (int k = na; k <= nb; ++k) st = st + c.T(k) * P.dpr2[k];
   for (int k = na; k <= nb; ++k) sd = sd + P.dpr2[k];
@@ -621,7 +642,8 @@ __device__ void ts_mix(const Dev &P, long long q2, Col &c, double *rhoa, double 
   if (nb < P.nk) rhob[nb] = c.P1(nb + 1) * c.T(nb) + c.P2(nb + 1) * c.S(nb);
 }
 
-__device__ void ts_convect(const Dev &P, long long q2, int nlev, Col c) {
+template <typename R>
+__device__ void ts_convect(const DevT<R> &P, long long q2, int nlev, Col c) {
   double rhoa[PCOM_MAXK + 2], rhob[PCOM_MAXK + 2];
   for (int k = 0; k <= P.nk + 1; ++k) { rhoa[k] = 0.0; rhob[k] = 0.0; }
   for (int k = 2; k <= nlev; ++k) rhoa[k] = c.P1(k) * c.T(k) + c.P2(k) * c.S(k);
@@ -655,9 +677,11 @@ __device__ void ts_convect(const Dev &P, long long q2, int nlev, Col c) {
   }
 }
 
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_ts(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
   double *tcs = sh, *scs = sh + nk * TB_X, *p1s = sh + 2 * nk * TB_X, *p2s = sh + 3 * nk * TB_X;
@@ -667,101 +691,102 @@ __global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P0, cons
   const int tx = threadIdx.x;
   const long long q2 = ok ? I2(P, i, j) : 0;
   const int ni = P.ni;
-  const double g = P.c.g;
+  const R g = P.c.g;
   if (threadIdx.y == 0) unstable[tx] = 0;
-  const double grho = g * P.c.rho0;
+  const R grho = g * P.c.rho0;
   const bool nrow = j <= P.njm, srow = j >= 2;
   const long long qw = q2 - 1, qs = q2 - ni, qsw = qs - 1, qe = q2 + 1, qn = q2 + ni;
   const int lev = ok ? P.lev_t[q2] : 0;
   for (int k = threadIdx.y + 1; k <= nk && ok; k += TB_K) {
     const int lw = P.lev_t[qw], le = P.lev_t[qe], ln = nrow ? P.lev_t[qn] : 0, ls = srow ? P.lev_t[qs] : 0;
-    const double rh4c = RH(4, j), rh4s = srow ? RH(4, j - 1) : 0.0;
+    const R rh4c = RH(4, j), rh4s = srow ? RH(4, j - 1) : 0.0;
     // sch (op_adv_ts) at U (i, j), (i-1, j), (i, j-1), (i-1, j-1)
-    const double sc_c = ld(P.sch_r, q2), sc_w = ld(P.sch_r, qw);
-    const double sc_s = srow ? ld(P.sch_r, qs) : 0.0, sc_sw = srow ? ld(P.sch_r, qsw) : 0.0;
-    const double r3c = RH(3, j), r3s = srow ? RH(3, j - 1) : 0.0;
+    const R sc_c = ld(P.sch_r, q2), sc_w = ld(P.sch_r, qw);
+    const R sc_s = srow ? ld(P.sch_r, qs) : 0.0, sc_sw = srow ? ld(P.sch_r, qsw) : 0.0;
+    const R r3c = RH(3, j), r3s = srow ? RH(3, j - 1) : 0.0;
     // ter(mch) to E (i-1, j), (i, j) and to N (i, j-1), (i, j)
-    const double mc = ld(P.mch, q2), me = ld(P.mch, qe), mw = ld(P.mch, qw);
-    const double mn = nrow ? ld(P.mch, qn) : 0.0, ms = srow ? ld(P.mch, qs) : 0.0;
-    const double c1c = 0.5 * (mc + me), c1w = 0.5 * (mw + mc);
-    const double c2c = nrow ? 0.5 * (mc + mn) : 0.0, c2s = srow ? 0.5 * (ms + mc) : 0.0;
-    const double bc = (double)P.bc;
+    const R mc = ld(P.mch, q2), me = ld(P.mch, qe), mw = ld(P.mch, qw);
+    const R mn = nrow ? ld(P.mch, qn) : 0.0, ms = srow ? ld(P.mch, qs) : 0.0;
+    const R c1c = 0.5 * (mc + me), c1w = 0.5 * (mw + mc);
+    const R c2c = nrow ? 0.5 * (mc + mn) : 0.0, c2s = srow ? 0.5 * (ms + mc) : 0.0;
+    const R bc = (R)P.bc;
     const long long o = P.n2 * (k - 1), q = q2 + o;
-    const double m_c = (double)(lev >= k), m_w = (double)(lw >= k), m_e = (double)(le >= k);
-    const double m_n = (double)(ln >= k), m_s = (double)(ls >= k);
-    const double m_k1 = (double)(lev >= k + 1), m_km = (double)(lev >= k - 1);
+    const R m_c = (R)(lev >= k), m_w = (R)(lw >= k), m_e = (R)(le >= k);
+    const R m_n = (R)(ln >= k), m_s = (R)(ls >= k);
+    const R m_k1 = (R)(lev >= k + 1), m_km = (R)(lev >= k - 1);
     // mass-weighted velocity: um1 = uc*sch on U, um2 = vc*sch*rh3
-    const double um1c = ld(P.uc, q) * sc_c, um1w = ld(P.uc, qw + o) * sc_w;
-    const double um1s = srow ? ld(P.uc, qs + o) * sc_s : 0.0, um1sw = srow ? ld(P.uc, qsw + o) * sc_sw : 0.0;
-    const double um2c = ld(P.vc, q) * sc_c * r3c, um2w = ld(P.vc, qw + o) * sc_w * r3c;
-    const double um2s = srow ? ld(P.vc, qs + o) * sc_s * r3s : 0.0;
-    const double um2sw = srow ? ld(P.vc, qsw + o) * sc_sw * r3s : 0.0;
+    const R um1c = ld(P.uc, q) * sc_c, um1w = ld(P.uc, qw + o) * sc_w;
+    const R um1s = srow ? ld(P.uc, qs + o) * sc_s : 0.0, um1sw = srow ? ld(P.uc, qsw + o) * sc_sw : 0.0;
+    const R um2c = ld(P.vc, q) * sc_c * r3c, um2w = ld(P.vc, qw + o) * sc_w * r3c;
+    const R um2s = srow ? ld(P.vc, qs + o) * sc_s * r3s : 0.0;
+    const R um2sw = srow ? ld(P.vc, qsw + o) * sc_sw * r3s : 0.0;
     // ter U->E (ns, sj=1) at (i, j), (i-1, j); ter U->N (ew, si=1) at (i, j), (i, j-1)
-    const double wa1c = srow ? 0.5 * (um1s + um1c) : 0.0, wa1w = srow ? 0.5 * (um1sw + um1w) : 0.0;
-    const double wa2c = 0.5 * (um2w + um2c), wa2s = srow ? 0.5 * (um2sw + um2s) : 0.0;
-    const double wmk = ld(P.wm, q), wmk1 = ld(P.wm, q + P.n2);  // wm has nkp levels
-    auto adv = [&](const double *var) -> double {
-      const double xc = ld(var, q), xe = ld(var, qe + o), xw = ld(var, qw + o);
-      const double xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
-      const double xkm = (k > 1) ? ld(var, q - P.n2) : 0.0, xk1 = (k < nk) ? ld(var, q + P.n2) : 0.0;
-      const double w1c = DIVX(xe - xc, 2, i), w1w = DIVX(xc - xw, 2, i - 1);
-      const double wb1 = 0.5 * (wa1w * w1w + wa1c * w1c);
-      double ans = DIVARH(wb1, 1, j);
-      const double w2c = nrow ? DIVY(xn - xc, 4, j) : 0.0;
-      double wb2 = 0.0;
+    const R wa1c = srow ? 0.5 * (um1s + um1c) : 0.0, wa1w = srow ? 0.5 * (um1sw + um1w) : 0.0;
+    const R wa2c = 0.5 * (um2w + um2c), wa2s = srow ? 0.5 * (um2sw + um2s) : 0.0;
+    const R wmk = ld(P.wm, q), wmk1 = ld(P.wm, q + P.n2);  // wm has nkp levels
+    auto adv = [&](const R *var) -> R {
+      const R xc = ld(var, q), xe = ld(var, qe + o), xw = ld(var, qw + o);
+      const R xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
+      const R xkm = (k > 1) ? ld(var, q - P.n2) : 0.0, xk1 = (k < nk) ? ld(var, q + P.n2) : 0.0;
+      const R w1c = DIVX(xe - xc, 2, i), w1w = DIVX(xc - xw, 2, i - 1);
+      const R wb1 = 0.5 * (wa1w * w1w + wa1c * w1c);
+      R ans = DIVARH(wb1, 1, j);
+      const R w2c = nrow ? DIVY(xn - xc, 4, j) : 0.0;
+      R wb2 = 0.0;
       if (srow) {
-        const double w2s = DIVY(xc - xs, 4, j - 1);
+        const R w2s = DIVY(xc - xs, 4, j - 1);
         wb2 = 0.5 * (wa2s * w2s + wa2c * w2c);
       }
       ans = ans + DIVARH(wb2, 1, j);
       // vter(wm * dx3(var)) / dpr
-      const double wmp_k = (k >= 2) ? wmk * (xkm - xc) : wmk * 0.0;
-      const double wmp_k1 = (k < nk) ? wmk1 * (xc - xk1) : wmk1 * 0.0;
+      const R wmp_k = (k >= 2) ? wmk * (xkm - xc) : wmk * 0.0;
+      const R wmp_k1 = (k < nk) ? wmk1 * (xc - xk1) : wmk1 * 0.0;
       ans = ans + DIVDP((wmp_k + wmp_k1) * 0.5, k);
       return ans;
     };
-    auto dif = [&](const double *var) -> double {
-      const double xc = ld(var, q), xe = ld(var, qe + o), xw = ld(var, qw + o);
-      const double xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
-      const double xkm = (k > 1) ? ld(var, q - P.n2) : 0.0, xk1 = (k < nk) ? ld(var, q + P.n2) : 0.0;
-      const double w1c = DIVARH(DIVX((xe - xc) * m_e * m_c, 2, i), 2, j);
-      const double w1w = DIVARH(DIVX((xc - xw) * m_c * m_w, 2, i - 1), 2, j);
-      const double A = DIVX(c1c * w1c - c1w * w1w, 1, i);
-      const double w2c = nrow ? DIVA(DIVY((xn - xc) * m_n * m_c, 4, j)) : 0.0;
-      double B = 0.0;
+    auto dif = [&](const R *var) -> R {
+      const R xc = ld(var, q), xe = ld(var, qe + o), xw = ld(var, qw + o);
+      const R xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
+      const R xkm = (k > 1) ? ld(var, q - P.n2) : 0.0, xk1 = (k < nk) ? ld(var, q + P.n2) : 0.0;
+      const R w1c = DIVARH(DIVX((xe - xc) * m_e * m_c, 2, i), 2, j);
+      const R w1w = DIVARH(DIVX((xc - xw) * m_c * m_w, 2, i - 1), 2, j);
+      const R A = DIVX(c1c * w1c - c1w * w1w, 1, i);
+      const R w2c = nrow ? DIVA(DIVY((xn - xc) * m_n * m_c, 4, j)) : 0.0;
+      R B = 0.0;
       if (srow) {
-        const double w2s = DIVA(DIVY((xc - xs) * m_c * m_s, 4, j - 1));
+        const R w2s = DIVA(DIVY((xc - xs) * m_c * m_s, 4, j - 1));
         B = DIVY((c2c * w2c) * rh4c - (c2s * w2s) * rh4s, 1, j);
       }
-      double ans = P.c.ah_c * DIVARH(A + B, 1, j);
-      double wkp_k = 0.0, wkp_k1 = 0.0;
+      R ans = P.c.ah_c * DIVARH(A + B, 1, j);
+      R wkp_k = 0.0, wkp_k1 = 0.0;
       if (k >= 2) {
-        const double pz = dvr((xkm - xc) * m_km * m_c, P.dz1[k], P.rdz1[k]);
+        const R pz = dvr((xkm - xc) * m_km * m_c, P.dz1[k], P.rdz1[k]);
         wkp_k = grho * ld(P.kh, q2 + P.n2 * (k - 1)) * pz;
       }
       if (k < nk) {
-        const double pz = dvr((xc - xk1) * m_c * m_k1, P.dz1[k + 1], P.rdz1[k + 1]);
+        const R pz = dvr((xc - xk1) * m_c * m_k1, P.dz1[k + 1], P.rdz1[k + 1]);
         wkp_k1 = grho * ld(P.kh, q2 + P.n2 * k) * pz;
       }
       ans = ans + DIVDP(wkp_k - wkp_k1, k);
       return ans;
     };
-    const double at = adv(P.tc), as = adv(P.sc);
-    const double dt_ = dif(P.tp), ds_ = dif(P.sp);
-    double p1 = -at, p2 = -as;
+    const R at = adv(P.tc), as = adv(P.sc);
+    const R dt_ = dif(P.tp), ds_ = dif(P.sp);
+    R p1 = -at, p2 = -as;
     p1 = p1 + dt_;
     p2 = p2 + ds_;
     if (k == 1) {
       p1 = p1 + DIVDP(P.c.gamma_t * (ld(P.bnd_t, q2) - ld(P.tc, q)) * m_c, 1);
       p2 = p2 + P.c.gamma_s * (ld(P.bnd_s, q2) - ld(P.sc, q)) * m_c * mc;
     }
+    // the tracer update in FP64 (mixed path: FP32 tendency, FP64 sum)
     const double rmc = ld(P.rmch, q2);
-    double tn = ld(P.tp, q) + dvr(p1 * bc * m_c, mc, rmc);
-    const double sn = ld(P.sp, q) + dvr(p2 * bc * m_c, mc, rmc);
+    double tn = (double)ld(P.tp, q) + dvr((double)(p1 * bc * m_c), (double)mc, rmc);
+    const double sn = (double)ld(P.sp, q) + dvr((double)(p2 * bc * m_c), (double)mc, rmc);
     if (m_c > 0 && tn < P.c.tice) tn = P.c.tice;
     tcs[(k - 1) * TB_X + tx] = tn;
     scs[(k - 1) * TB_X + tx] = sn;
-    const double2 pr = P.prho[q];
+    const auto pr = P.prho[q];
     p1s[(k - 1) * TB_X + tx] = pr.x;
     p2s[(k - 1) * TB_X + tx] = pr.y;
   }
@@ -798,9 +823,11 @@ __global__ void __launch_bounds__(512) k_ts(const __grid_constant__ Dev P0, cons
 
 // ----------------------------------------------------------------------------
 // den_prho (mod_den.f90:120-153)
-template <bool BATCH>
-__global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps) {
-  const Dev &P = BATCH ? Ps[blockIdx.z] : P0;
+template <typename R, bool BATCH>
+__global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  constexpr bool MIXED = std::is_same<R, float>::value;
+  (void)MIXED;
   int i, j;
   if (!cell(P, i, j, false)) return;
   const long long q2 = I2(P, i, j);
@@ -811,7 +838,7 @@ __global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ Dev P0
     const long long q = q2 + P.n2 * (k - 1);
     const double t = P.tc[q], s = P.sc[q], p = ch * P.pr2[k];
     double ra = den_rho(P.c, t + dt, s, p), rb = den_rho(P.c, t - dt, s, p);
-    double2 r;
+    typename Vec2<R>::type r;
     r.x = (ra - rb) / (2 * dt);
     ra = den_rho(P.c, t, s + ds, p);
     rb = den_rho(P.c, t, s - ds, p);
@@ -830,39 +857,65 @@ static const dim3 kBlock3(TB_X, TB_K, 1);
 static inline dim3 g3(int nx, int ny, int nz) { return dim3((nx + TB_X - 1) / TB_X, ny, nz); }
 static inline size_t sm3(int nk, int planes) { return (size_t)planes * nk * TB_X * sizeof(double); }
 
-void launch_alpha_tobot(const Dev &P, cudaStream_t s) { k_alpha_tobot<false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
-void launch_pgra2d(const Dev &P, cudaStream_t s) { k_pgra2d<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
-void launch_uv2d(const Dev &P, int mode, cudaStream_t s) {
-  k_uv2d<false><<<dim3((P.glo_ni + 31) / 32, (P.nj + 3) / 4), dim3(32, 4), 0, s>>>(P, nullptr, mode);
+template <typename R>
+void launch_alpha_tobot(const DevT<R> &P, cudaStream_t s) { k_alpha_tobot<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+template <typename R>
+void launch_pgra2d(const DevT<R> &P, cudaStream_t s) { k_pgra2d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
+template <typename R>
+void launch_uv2d(const DevT<R> &P, int mode, cudaStream_t s) {
+  k_uv2d<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj + 3) / 4), dim3(32, 4), 0, s>>>(P, nullptr, mode);
 }
-void launch_upwelling(const Dev &P, int with_acw, cudaStream_t s) {
-  k_upwelling<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 3), s>>>(P, nullptr, with_acw);
+template <typename R>
+void launch_upwelling(const DevT<R> &P, int with_acw, cudaStream_t s) {
+  k_upwelling<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 3), s>>>(P, nullptr, with_acw);
 }
-void launch_readyc3d(const Dev &P, cudaStream_t s) { k_readyc3d<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr); }
-void launch_clin(const Dev &P, cudaStream_t s) {
-  k_clin<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2) + 2 * TB_X * sizeof(double), s>>>(P, nullptr);
+template <typename R>
+void launch_readyc3d(const DevT<R> &P, cudaStream_t s) { k_readyc3d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr); }
+template <typename R>
+void launch_clin(const DevT<R> &P, cudaStream_t s) {
+  k_clin<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2) + 2 * TB_X * sizeof(double), s>>>(P, nullptr);
 }
-void launch_smag(const Dev &P, cudaStream_t s) {
-  if (P.nj > 2) k_smag<false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, 1), dim3(32, 4), 0, s>>>(P, nullptr);
+template <typename R>
+void launch_smag(const DevT<R> &P, cudaStream_t s) {
+  if (P.nj > 2) k_smag<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, 1), dim3(32, 4), 0, s>>>(P, nullptr);
 }
-void launch_ssh(const Dev &P, cudaStream_t s) { k_ssh<false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
-void launch_ts(const Dev &P, cudaStream_t s) { k_ts<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
-void launch_den_prho(const Dev &P, cudaStream_t s) { k_den_prho<false><<<g3(P.ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr); }
+template <typename R>
+void launch_ssh(const DevT<R> &P, cudaStream_t s) { k_ssh<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+template <typename R>
+void launch_ts(const DevT<R> &P, cudaStream_t s) { k_ts<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
+template <typename R>
+void launch_den_prho(const DevT<R> &P, cudaStream_t s) { k_den_prho<R, false><<<g3(P.ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr); }
+
+
+#define PCOM_INST(R)                                                   \
+  template void launch_alpha_tobot<R>(const DevT<R> &, cudaStream_t); \
+  template void launch_pgra2d<R>(const DevT<R> &, cudaStream_t);      \
+  template void launch_uv2d<R>(const DevT<R> &, int, cudaStream_t);   \
+  template void launch_upwelling<R>(const DevT<R> &, int, cudaStream_t); \
+  template void launch_readyc3d<R>(const DevT<R> &, cudaStream_t);    \
+  template void launch_clin<R>(const DevT<R> &, cudaStream_t);        \
+  template void launch_smag<R>(const DevT<R> &, cudaStream_t);        \
+  template void launch_ssh<R>(const DevT<R> &, cudaStream_t);         \
+  template void launch_ts<R>(const DevT<R> &, cudaStream_t);          \
+  template void launch_den_prho<R>(const DevT<R> &, cudaStream_t);
+PCOM_INST(double)
+PCOM_INST(float)
+#undef PCOM_INST
 
 void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cudaStream_t s) {
   Dev none{};  // the by-value parameter is unused in the batched form
   const int n = b.n;
   switch (kernel) {
-  case BK_ALPHA_TOBOT: k_alpha_tobot<true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
-  case BK_PGRA2D: k_pgra2d<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
-  case BK_UV2D: k_uv2d<true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs, arg); break;
-  case BK_UPWELLING: k_upwelling<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 3), s>>>(none, dPs, arg); break;
-  case BK_READYC3D: k_readyc3d<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2), s>>>(none, dPs); break;
-  case BK_CLIN: k_clin<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
-  case BK_SMAG: k_smag<true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
-  case BK_SSH: k_ssh<true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
-  case BK_TS: k_ts<true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
-  case BK_DEN_PRHO: k_den_prho<true><<<g3(b.ni, b.nj, n), kBlock3, 0, s>>>(none, dPs); break;
+  case BK_ALPHA_TOBOT: k_alpha_tobot<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
+  case BK_PGRA2D: k_pgra2d<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
+  case BK_UV2D: k_uv2d<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs, arg); break;
+  case BK_UPWELLING: k_upwelling<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 3), s>>>(none, dPs, arg); break;
+  case BK_READYC3D: k_readyc3d<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2), s>>>(none, dPs); break;
+  case BK_CLIN: k_clin<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
+  case BK_SMAG: k_smag<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
+  case BK_SSH: k_ssh<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
+  case BK_TS: k_ts<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
+  case BK_DEN_PRHO: k_den_prho<double, true><<<g3(b.ni, b.nj, n), kBlock3, 0, s>>>(none, dPs); break;
   default: break;
   }
 }

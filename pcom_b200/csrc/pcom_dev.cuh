@@ -1,7 +1,8 @@
 // pcom_dev.cuh -- device-side view of one PCOM domain and the helpers every
 // kernel shares.
 //
-// Layout in HBM: every field is FP64, Fortran order (i fastest) over the
+// Layout in HBM: every field is FP64 (the mixed path stores its 3-D fields
+// as FP32), Fortran order (i fastest) over the
 // padded ni x nj domain, one contiguous plane per level.  The two x-halo
 // columns (1 and ni) of every stored field hold copies of columns ni-1 and 2:
 // that is what the reference's halo exchange leaves behind after each
@@ -17,6 +18,7 @@
 // reference's gfortran build on x86-64 (SSE2, no FMA).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #define PCOM_MAXK 64
@@ -28,37 +30,38 @@ struct DevConsts {
 };
 
 // Everything a kernel needs, passed by value as a __grid_constant__ param.
-struct Dev {
+// R is the storage type of the 3-D fields: double for the FP64 path, float
+// for the mixed path (whose 2-D fields, barotropic state and accumulations
+// stay double).
+template <typename R> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// Fields of every precision: sizes, constants, the static grid, the 2-D
+// state and scratch (always FP64).
+struct DevCommon {
   int ni, nj, nk, nkp, nim, njm, glo_ni, glo_nj;
   int bt, bc, nstep, rst;
   long long n2, n3, n3p;
   DevConsts c;
   double pr2[PCOM_MAXK], dpr2[PCOM_MAXK], dz1[PCOM_MAXK + 1];  // 1-based: [k]
+  double dz2[PCOM_MAXK];                                         // layer thickness (gi2), 1-based
   // static 2D (index 1..4 = grid g1j..g4j)
   const double *rh[5], *dxx[5], *dxy[5];
   const double *tn3;
   const int *lev_t, *lev_u;
   const double *prh_t, *phih_t, *prh_u;
   const double *cv1, *cv2, *cor, *graphihx, *graphihy;
-  const double *km, *kh;  // nkp levels
   // forcing (bnd)
   const double *taux, *tauy, *bnd_t, *bnd_s, *bnd_pa;
-  // state
-  double *tc, *sc, *tp, *sp;
-  double *uc, *vc, *up, *vp;
-  double *auc, *aup, *aupp, *avc, *avp, *avpp;
+  // 2-D state
   double *ubc, *vbc, *ubp, *vbp;
   double *chc, *chp, *mch, *mch2;
-  double *am, *alpha, *adp, *wm;
-  double2 *prho;
-  // step intermediates
-  double *fx, *fy, *pax, *pay, *ut, *vt;
+  // 2-D step intermediates
+  double *pax, *pay, *ut, *vt;
   double *bphi[4], *bgra[4];  // xn, xs, ye, yw
   double *sch_r, *sch_w;      // readyc sch (land 1) and upwelling sqrt(ter(chp))
-  double *uu, *vv;            // unweighted velocity for smag
-  double *tn_, *sn_;          // new T/S (int_ts writes here, then pointers rotate)
-  // accumulators
-  double *act, *acs, *acr, *acu, *acv, *acw, *acch, *acssh;
+  double *acch, *acssh;
   // barotropic subcycle scratch
   double *tr_ch[2], *tr_ub[2], *tr_vb[2];
   double *tr_acc[6];  // mch, mch2, ub, vb accumulators; first-substep viscosity (u, v)
@@ -85,17 +88,48 @@ struct Dev {
   double *rsch, *rsch2, *rchc, *rmch, *rgm2, *schc, *schu, *rmch2;
   // AB3 start-up control for the current step
   int ab3_mode;    // 0 normal, 1 step 1 (copy auc into aup, aupp), 2 step 2 (aupp = aup)
+  // mixed path: alpha and adp are stored as anomalies from the reference
+  // profile alpha_r(k) = 1/rho(T_r(k), S_r(k), pr(k)) and from its int_tobot
+  // over the column's own wet levels (adp_ref below, from the suffix sums
+  // adp_cum(k) = sum_{kk >= k} alpha_r(kk) dpr(kk)); 1-based.  am1 is an
+  // FP64 copy of am at level 1 for the barotropic subcycle
+  double alpha_r[PCOM_MAXK], adp_cum[PCOM_MAXK + 1];
+  double *am1;
 };
+
+// The 3-D fields, stored as R.
+template <typename R>
+struct DevT : DevCommon {
+  const R *km, *kh;  // nkp levels
+  R *tc, *sc, *tp, *sp;
+  R *uc, *vc, *up, *vp;
+  R *auc, *aup, *aupp, *avc, *avp, *avpp;
+  R *am, *alpha, *adp, *wm;
+  typename Vec2<R>::type *prho;
+  R *fx, *fy;
+  R *uu, *vv;                 // unweighted velocity for smag
+  R *tn_, *sn_;               // new T/S (int_ts writes here, then pointers rotate)
+  R *act, *acs, *acr, *acu, *acv, *acw;  // accumulators
+};
+
+using Dev = DevT<double>;
+using DevM = DevT<float>;
+
 
 #define PD __device__ __forceinline__
 
-PD long long I2(const Dev &P, int i, int j) { return (long long)(i - 1) + (long long)P.ni * (j - 1); }
-PD long long I3(const Dev &P, int i, int j, int k) { return I2(P, i, j) + P.n2 * (k - 1); }
+template <typename R>
+PD long long I2(const DevT<R> &P, int i, int j) { return (long long)(i - 1) + (long long)P.ni * (j - 1); }
+template <typename R>
+PD long long I3(const DevT<R> &P, int i, int j, int k) { return I2(P, i, j) + P.n2 * (k - 1); }
 // ring neighbours of an interior column (2 <= i <= ni-1)
-PD int IM(const Dev &P, int i) { return i == 2 ? P.ni - 1 : i - 1; }
-PD int IP(const Dev &P, int i) { return i == P.ni - 1 ? 2 : i + 1; }
+template <typename R>
+PD int IM(const DevT<R> &P, int i) { return i == 2 ? P.ni - 1 : i - 1; }
+template <typename R>
+PD int IP(const DevT<R> &P, int i) { return i == P.ni - 1 ? 2 : i + 1; }
 
 PD double ld(const double *p, long long q) { return __ldg(p + q); }
+PD float ld(const float *p, long long q) { return __ldg(p + q); }
 
 // x / y rounded to nearest, given ry = 1/y correctly rounded: the quotient
 // estimate x*ry is corrected once with its exact remainder (Markstein's
@@ -108,12 +142,44 @@ PD double dvr(double x, double y, double ry) {
   const double r = __fma_rn(-q, y, x);
   return __fma_rn(r, ry, q);
 }
+// mixed path: an FP32 quotient from the (rounded) reciprocal
+template <typename Y, typename RY>
+PD float dvr(float x, Y, RY ry) { return x * (float)ry; }
+
+// alpha and adp as stored (anomalies on the mixed path) and as used
+template <typename R>
+PD R alpha_store(const DevT<R> &P, double v, int k) {
+  if constexpr (std::is_same<R, float>::value) return (float)(v - P.alpha_r[k]); else return v;
+}
+template <typename R>
+PD double alpha_full(const DevT<R> &P, R v, int k) {
+  if constexpr (std::is_same<R, float>::value) return P.alpha_r[k] + (double)v; else return v;
+}
+// int_tobot of the reference profile over levels k..lev of a column
+PD double adp_ref(const double *alpha_r, const double *dpr2, const double *cum, int k, int lev) {
+  return k <= lev ? alpha_r[k] * dpr2[k] * 0.5 + (cum[k + 1] - cum[lev + 1]) : 0.0;
+}
+// q2: the column's 2-D index (its lev sets the reference)
+template <typename R>
+PD R adp_store(const DevT<R> &P, double v, int k, long long q2) {
+  if constexpr (std::is_same<R, float>::value)
+    return (float)(v - adp_ref(P.alpha_r, P.dpr2, P.adp_cum, k, __ldg(P.lev_t + q2)));
+  else return v;
+}
+template <typename R>
+PD double adp_full(const DevT<R> &P, R v, int k, long long q2) {
+  if constexpr (std::is_same<R, float>::value)
+    return adp_ref(P.alpha_r, P.dpr2, P.adp_cum, k, __ldg(P.lev_t + q2)) + (double)v;
+  else return v;
+}
 
 // store to an interior column and to its halo twin
-PD void st2(double *p, const Dev &P, int i, long long q, double v) {
-  p[q] = v;
-  if (i == 2) p[q + (P.ni - 2)] = v;
-  else if (i == P.ni - 1) p[q - (P.ni - 2)] = v;
+template <typename T, typename R, typename V>
+PD void st2(T *p, const DevT<R> &P, int i, long long q, V v) {
+  const T w = (T)v;
+  p[q] = w;
+  if (i == 2) p[q + (P.ni - 2)] = w;
+  else if (i == P.ni - 1) p[q - (P.ni - 2)] = w;
 }
 
 // den_rho, mod_den.f90:57-118, same evaluation order as the reference.
@@ -148,7 +214,8 @@ PD double den_rho(const DevConsts &C, double t, double s, double p0) {
 
 // ter T->U, diagonal 4-point mean (ter_r2d, hga = g1j, mod_op.f90:416-419);
 // rows j = nj get the default `dft`.
-PD double terTU(const Dev &P, const double *f, int i, int j, double dft) {
+template <typename R>
+PD double terTU(const DevT<R> &P, const double *f, int i, int j, double dft) {
   if (j > P.njm) return dft;
   long long q = I2(P, i, j);
   return (ld(f, q) + ld(f, q + P.ni) + ld(f, q + 1) + ld(f, q + 1 + P.ni)) * 0.25;
@@ -157,8 +224,10 @@ PD double terTU(const Dev &P, const double *f, int i, int j, double dft) {
 // msk of the T grid (g12) and U grid (g32): set_grid builds msk = (lev >= k)
 // (main.f90:605-625); pcom_gpu_upload_static checks that the given masks are
 // exactly that, so kernels derive them from the 2-D lev arrays.
-PD double mT(const Dev &P, long long q2, int k) { return (double)(__ldg(P.lev_t + q2) >= k); }
-PD double mU(const Dev &P, long long q2, int k) { return (double)(__ldg(P.lev_u + q2) >= k); }
+template <typename R>
+PD double mT(const DevT<R> &P, long long q2, int k) { return (double)(__ldg(P.lev_t + q2) >= k); }
+template <typename R>
+PD double mU(const DevT<R> &P, long long q2, int k) { return (double)(__ldg(P.lev_u + q2) >= k); }
 
 // launch geometry shared by the column kernels
 #define COLS_X 32

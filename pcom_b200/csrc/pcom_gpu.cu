@@ -90,7 +90,8 @@ void make_consts(bool r8, DevConsts &c) {
 }
 
 // ------------------------------------------------------------------- kernels
-__global__ void k_nonfinite(const double *f, const int *lev, int nk, long long n2, int planes,
+template <typename T>
+__global__ void k_nonfinite(const T *f, const int *lev, int nk, long long n2, int planes,
                             unsigned long long *count) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = n2 * planes;
@@ -104,6 +105,84 @@ __global__ void k_nonfinite(const double *f, const int *lev, int nk, long long n
   if (c) atomicAdd(count, c);
 }
 
+// mixed path: conversions between the FP64 host layout and FP32 device
+// storage; kind 1 subtracts / adds a per-level profile (alpha, adp anomalies)
+// (kind 1: alpha, a per-level profile; kind 2: adp, the profile's int_tobot
+// over each column's wet levels, which needs lev)
+struct Profile {
+  double alpha_r[PCOM_MAXK], dpr2[PCOM_MAXK], cum[PCOM_MAXK + 1];
+  const int *lev;
+};
+__device__ double profile_at(const Profile &pr, long long p, long long n2, int per, int kind) {
+  const long long pt = p / per;
+  const int k = (int)(pt / n2) + 1;
+  if (kind == 1) return pr.alpha_r[k];
+  if (kind == 2) return adp_ref(pr.alpha_r, pr.dpr2, pr.cum, k, pr.lev[pt % n2]);
+  return 0.0;
+}
+__global__ void k_to_f32(const double *src, float *dst, long long n, long long n2, int per, int kind,
+                         const __grid_constant__ Profile pr) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    double v = src[p];
+    if (kind) v -= profile_at(pr, p, n2, per, kind);
+    dst[p] = (float)v;
+  }
+}
+__global__ void k_to_f64(const float *src, double *dst, long long n, long long n2, int per, int kind,
+                         const __grid_constant__ Profile pr) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    double v = (double)src[p];
+    if (kind) v += profile_at(pr, p, n2, per, kind);
+    dst[p] = v;
+  }
+}
+
+// reference profile of the mixed path: alpha_r(k) = 1/rho(T_r, S_r, pr(k))
+__global__ void k_ref_profile(DevConsts c, const double *tr, const double *sr, const double *pr, int nk, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int k = 1; k <= nk; ++k) out[k] = 1.0 / den_rho(c, tr[k], sr[k], pr[k]);
+}
+
+// global sums: wet volume, and the volume integrals of T and S over T cells
+// of interior columns and rows; fixed-order reduction (deterministic)
+template <typename R>
+__global__ void k_sums(const __grid_constant__ DevT<R> P, double *part) {
+  __shared__ double sh[3][256];
+  double v = 0.0, t = 0.0, s = 0.0;
+  const long long nint = (long long)P.glo_ni * (P.nj - 2) * P.nk;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < nint; p += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(p % P.glo_ni);
+    const int j = (int)((p / P.glo_ni) % (P.nj - 2)) + 2;
+    const int k = (int)(p / ((long long)P.glo_ni * (P.nj - 2))) + 1;
+    const long long q2 = (long long)(x + 1) + (long long)P.ni * (j - 1);
+    if (P.lev_t[q2] < k) continue;
+    const double area = (P.c.a * P.rh[1][q2] * P.dxx[1][q2]) * (P.c.a * P.dxy[1][q2]);
+    const double dv = area * P.dz2[k];
+    const long long q = q2 + P.n2 * (k - 1);
+    v += dv;
+    t += (double)P.tc[q] * dv;
+    s += (double)P.sc[q] * dv;
+  }
+  sh[0][threadIdx.x] = v;
+  sh[1][threadIdx.x] = t;
+  sh[2][threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) part[3 * blockIdx.x + c] = sh[c][0];
+}
+__global__ void k_sums_final(const double *part, int nb, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < 3; ++c) a[c] += part[3 * b + c];
+  for (int c = 0; c < 3; ++c) out[c] = a[c];
+}
+
 struct ProfEntry {
   long long launches = 0;
   double ms = 0.0;
@@ -114,7 +193,7 @@ struct ProfEntry {
 
 void launch_nonfinite(const double *f, const int *lev, int nk, long long n2, int planes, unsigned long long *count,
                       cudaStream_t s) {
-  k_nonfinite<<<592, 256, 0, s>>>(f, lev, nk, n2, planes, count);
+  k_nonfinite<double><<<592, 256, 0, s>>>(f, lev, nk, n2, planes, count);
 }
 
 struct pcom_handle {
@@ -125,6 +204,15 @@ struct pcom_handle {
   bool own_stream = false;
   int device = 0;
   Dev D{};
+  // mixed path: the 3-D fields live in DM (FP32); D keeps the shared FP64
+  // part and serves the barotropic kernel (its am is the FP64 level-1 copy)
+  bool mixed = false;
+  DevM DM{};
+  float *ab_uf[3] = {}, *ab_vf[3] = {}, *t_poolf[3] = {}, *s_poolf[3] = {};
+  double *stage = nullptr;     // FP64 staging for host copies of FP32 fields
+  bool ref_set = false;        // reference profile of the anomalies fixed
+  double *d_sums = nullptr;    // global-sum partials and result
+  std::vector<int> lev_t_host;
   std::vector<void *> allocs;
   double *ab_u[3] = {}, *ab_v[3] = {};  // AB3 ring buffers: [ic], [ip], [ipp]
   int ic = 0, ip = 1, ipp = 2;
@@ -193,16 +281,24 @@ int sync_check(pcom_handle *h) {
   return PCOM_OK;
 }
 
-void bind_rotating(pcom_handle *h) {
-  Dev &D = h->D;
-  D.auc = h->ab_u[h->ic]; D.aup = h->ab_u[h->ip]; D.aupp = h->ab_u[h->ipp];
-  D.avc = h->ab_v[h->ic]; D.avp = h->ab_v[h->ip]; D.avpp = h->ab_v[h->ipp];
-  D.tc = h->t_pool[h->itc]; D.tp = h->t_pool[h->itp];
-  D.sc = h->s_pool[h->itc]; D.sp = h->s_pool[h->itp];
+template <typename R>
+void bind_ring(pcom_handle *h, DevT<R> &D, R *const *abu, R *const *abv, R *const *tp, R *const *sp) {
+  D.auc = abu[h->ic]; D.aup = abu[h->ip]; D.aupp = abu[h->ipp];
+  D.avc = abv[h->ic]; D.avp = abv[h->ip]; D.avpp = abv[h->ipp];
+  D.tc = tp[h->itc]; D.tp = tp[h->itp];
+  D.sc = sp[h->itc]; D.sp = sp[h->itp];
   int fr = 0;
   while (fr == h->itc || fr == h->itp) ++fr;
-  D.tn_ = h->t_pool[fr];
-  D.sn_ = h->s_pool[fr];
+  D.tn_ = tp[fr];
+  D.sn_ = sp[fr];
+}
+void bind_rotating(pcom_handle *h) {
+  if (h->mixed) bind_ring(h, h->DM, h->ab_uf, h->ab_vf, h->t_poolf, h->s_poolf);
+  else bind_ring(h, h->D, h->ab_u, h->ab_v, h->t_pool, h->s_pool);
+}
+// the mixed path's DM shares every FP64 field of D
+void sync_common(pcom_handle *h) {
+  if (h->mixed) static_cast<DevCommon &>(h->DM) = static_cast<const DevCommon &>(h->D);
 }
 
 int pick_trop_config(pcom_handle *h) {
@@ -244,25 +340,35 @@ int pick_trop_config(pcom_handle *h) {
   return PCOM_OK;
 }
 
-// ---- the pieces of the step
+// ---- the pieces of the step (FP64 handle: D; mixed handle: DM)
+#define ON_DEV(call_on) \
+  do {                  \
+    if (h->mixed) {     \
+      auto &X = h->DM;  \
+      call_on;          \
+    } else {            \
+      auto &X = h->D;   \
+      call_on;          \
+    }                   \
+  } while (0)
 int do_den_alpha(pcom_handle *h) {
   Prof p(h, "den_alpha+int_tobot");
-  launch_alpha_tobot(h->D, h->stream);
+  ON_DEV(launch_alpha_tobot(X, h->stream));
   return PCOM_OK;
 }
 int do_pgra(pcom_handle *h) {
   Prof p(h, "int_pgra");
-  launch_pgra2d(h->D, h->stream);
+  ON_DEV(launch_pgra2d(X, h->stream));
   return PCOM_OK;
 }
 int do_readyc(pcom_handle *h, int64_t iter) {
   {
     Prof p(h, "readyc_2d");
-    launch_uv2d(h->D, 0, h->stream);
+    ON_DEV(launch_uv2d(X, 0, h->stream));
   }
   {
     Prof p(h, "upwelling");
-    launch_upwelling(h->D, 0, h->stream);
+    ON_DEV(launch_upwelling(X, 0, h->stream));
   }
   // AB3 history: aupp <- aup <- auc (mod_int.f90:115-118) by rotation
   int old_pp = h->ipp;
@@ -271,17 +377,22 @@ int do_readyc(pcom_handle *h, int64_t iter) {
   h->ic = old_pp;
   bind_rotating(h);
   const bool fresh = h->dims.rst != 1;
-  h->D.ab3_mode = (fresh && iter == 1) ? 1 : 0;
+  h->D.ab3_mode = h->DM.ab3_mode = (fresh && iter == 1) ? 1 : 0;
   if (fresh && iter == 2) {
     // aupp = aup (mod_int.f90:128-130)
-    CK(cudaMemcpyAsync(h->D.aupp, h->D.aup, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->D.avpp, h->D.avp, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (h->mixed) {
+      CK(cudaMemcpyAsync(h->DM.aupp, h->DM.aup, h->n3 * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->DM.avpp, h->DM.avp, h->n3 * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+      CK(cudaMemcpyAsync(h->D.aupp, h->D.aup, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->D.avpp, h->D.avp, h->n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    }
   }
   {
     Prof p(h, "readyc_3d");
-    launch_readyc3d(h->D, h->stream);
+    ON_DEV(launch_readyc3d(X, h->stream));
   }
-  h->D.ab3_mode = 0;
+  h->D.ab3_mode = h->DM.ab3_mode = 0;
   return PCOM_OK;
 }
 int do_trop(pcom_handle *h) {
@@ -305,38 +416,38 @@ int do_trop(pcom_handle *h) {
 int do_clin(pcom_handle *h) {
   {
     Prof p(h, "clin_2d");
-    launch_uv2d(h->D, 2, h->stream);
+    ON_DEV(launch_uv2d(X, 2, h->stream));
   }
   {
     Prof p(h, "int_clin");
-    launch_clin(h->D, h->stream);
+    ON_DEV(launch_clin(X, h->stream));
   }
   {
     Prof p(h, "smag");
-    launch_smag(h->D, h->stream);
+    ON_DEV(launch_smag(X, h->stream));
   }
   h->n_uv++;
   return PCOM_OK;
 }
 int do_ssh(pcom_handle *h) {
   Prof p(h, "int_ssh");
-  launch_ssh(h->D, h->stream);
+  ON_DEV(launch_ssh(X, h->stream));
   h->n_ssh++;
   return PCOM_OK;
 }
 int do_ts(pcom_handle *h) {
   {
     Prof p(h, "ts_2d");
-    launch_uv2d(h->D, 1, h->stream);
+    ON_DEV(launch_uv2d(X, 1, h->stream));
   }
   {
     Prof p(h, "upwelling+acw");
-    launch_upwelling(h->D, 1, h->stream);
+    ON_DEV(launch_upwelling(X, 1, h->stream));
   }
   h->n_w++;
   {
     Prof p(h, "int_ts");
-    launch_ts(h->D, h->stream);
+    ON_DEV(launch_ts(X, h->stream));
   }
   // tc = tp = the buffer just written (mod_int.f90:496-497)
   int fr = 0;
@@ -383,9 +494,59 @@ int copy_out(pcom_handle *h, double *dst, const double *src, long long n) {
   return PCOM_OK;
 }
 
+// the 3-D fields of one storage type
+template <typename R>
+int alloc_3d(pcom_handle *h, DevT<R> &X, R **abu, R **abv, R **tpool, R **spool) {
+  const long long n3 = h->n3, n3p = h->n3p;
+  int rc = 0;
+  auto A = [&](R **p, long long n) { if (!rc) rc = h->alloc(p, (size_t)n); };
+  R *p = nullptr;
+  A(&p, n3p); X.km = p; A(&p, n3p); X.kh = p;
+  for (int q = 0; q < 3; ++q) { A(&tpool[q], n3); A(&spool[q], n3); A(&abu[q], n3); A(&abv[q], n3); }
+  A(&X.uc, n3); A(&X.vc, n3); A(&X.up, n3); A(&X.vp, n3);
+  A(&X.am, n3); A(&X.alpha, n3); A(&X.adp, n3); A(&X.wm, n3p);
+  {
+    typename Vec2<R>::type *pr = nullptr;
+    if (!rc) rc = h->alloc(&pr, (size_t)n3);
+    X.prho = pr;
+  }
+  A(&X.fx, n3); A(&X.fy, n3); A(&X.uu, n3); A(&X.vv, n3);
+  A(&X.act, n3); A(&X.acs, n3); A(&X.acr, n3); A(&X.acu, n3); A(&X.acv, n3); A(&X.acw, n3);
+  return rc;
+}
+
+// host FP64 array -> FP32 device array through the staging buffer
+Profile profile_of(const DevCommon &D) {
+  Profile pr{};
+  memcpy(pr.alpha_r, D.alpha_r, sizeof pr.alpha_r);
+  memcpy(pr.dpr2, D.dpr2, sizeof pr.dpr2);
+  memcpy(pr.cum, D.adp_cum, sizeof pr.cum);
+  pr.lev = D.lev_t;
+  return pr;
+}
+int put_f32(pcom_handle *h, float *dst, const double *src, long long n, int kind, int per = 1) {
+  CK(cudaMemcpyAsync(h->stage, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const Profile pr = profile_of(h->D);
+  k_to_f32<<<592, 256, 0, h->stream>>>(h->stage, dst, n, h->n2, per, kind, pr);
+  CK(cudaGetLastError());
+  return PCOM_OK;
+}
+// FP32 device array -> host FP64 array through the staging buffer
+int get_f32(pcom_handle *h, double *dst, const float *src, long long n, int kind, int per = 1) {
+  const Profile pr = profile_of(h->D);
+  k_to_f64<<<592, 256, 0, h->stream>>>(src, h->stage, n, h->n2, per, kind, pr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dst, h->stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return PCOM_OK;
+}
+
+// a named device array: FP64, or FP32 (mixed path) with its profile kind
 struct Named {
   const double *p;
   long long n;
+  const float *pf = nullptr;  // FP32 storage (then p is null)
+  int kind = 0;               // 1: alpha anomaly, 2: adp anomaly
+  int per = 1;                // values per point (prho: 2)
 };
 
 Named lookup(pcom_handle *h, const std::string &s) {
@@ -396,25 +557,140 @@ Named lookup(pcom_handle *h, const std::string &s) {
     if (s == std::string("bphi_") + b4[q]) return {D.bphi[q], n2};
     if (s == std::string("bgraphi_") + b4[q]) return {D.bgra[q], n2};
   }
-  const std::map<std::string, Named> m = {
-      {"tc", {D.tc, n3}},     {"sc", {D.sc, n3}},       {"tp", {D.tp, n3}},     {"sp", {D.sp, n3}},
-      {"uc", {D.uc, n3}},     {"vc", {D.vc, n3}},       {"up", {D.up, n3}},     {"vp", {D.vp, n3}},
-      {"auc", {D.auc, n3}},   {"aup", {D.aup, n3}},     {"aupp", {D.aupp, n3}}, {"avc", {D.avc, n3}},
-      {"avp", {D.avp, n3}},   {"avpp", {D.avpp, n3}},   {"ubc", {D.ubc, n2}},   {"vbc", {D.vbc, n2}},
-      {"ubp", {D.ubp, n2}},   {"vbp", {D.vbp, n2}},     {"chc", {D.chc, n2}},   {"chp", {D.chp, n2}},
-      {"mch", {D.mch, n2}},   {"mch2", {D.mch2, n2}},   {"am", {D.am, n3}},     {"alpha", {D.alpha, n3}},
-      {"adp", {D.adp, n3}},   {"wm", {D.wm, n3p}},      {"prho", {(const double *)D.prho, 2 * n3}},
-      {"fx", {D.fx, n3}},     {"fy", {D.fy, n3}},       {"pax", {D.pax, n2}},   {"pay", {D.pay, n2}},
-      {"ut", {D.ut, n2}},     {"vt", {D.vt, n2}},       {"act", {D.act, n3}},   {"acs", {D.acs, n3}},
-      {"acr", {D.acr, n3}},   {"acu", {D.acu, n3}},     {"acv", {D.acv, n3}},   {"acw", {D.acw, n3}},
-      {"acch", {D.acch, n2}}, {"acssh", {D.acssh, n2}}, {"km", {D.km, n3p}},    {"kh", {D.kh, n3p}},
-      {"cor", {D.cor, n2}},   {"cv1", {D.cv1, n2}},     {"cv2", {D.cv2, n2}},   {"graphihx", {D.graphihx, n2}},
-      {"graphihy", {D.graphihy, n2}}, {"sch_r", {D.sch_r, n2}}, {"sch_w", {D.sch_w, n2}},
-      {"bnd_taux", {D.taux, n2}}, {"bnd_tauy", {D.tauy, n2}}, {"bnd_t", {D.bnd_t, n2}}, {"bnd_s", {D.bnd_s, n2}},
-      {"bnd_pa", {D.bnd_pa, n2}}, {"uu", {D.uu, n3}}, {"vv", {D.vv, n3}}};
-  auto it = m.find(s);
-  if (it == m.end()) return {nullptr, 0};
-  return it->second;
+  const std::map<std::string, Named> m2 = {
+      {"ubc", {D.ubc, n2}},   {"vbc", {D.vbc, n2}},     {"ubp", {D.ubp, n2}},   {"vbp", {D.vbp, n2}},
+      {"chc", {D.chc, n2}},   {"chp", {D.chp, n2}},     {"mch", {D.mch, n2}},   {"mch2", {D.mch2, n2}},
+      {"pax", {D.pax, n2}},   {"pay", {D.pay, n2}},     {"ut", {D.ut, n2}},     {"vt", {D.vt, n2}},
+      {"acch", {D.acch, n2}}, {"acssh", {D.acssh, n2}}, {"cor", {D.cor, n2}},   {"cv1", {D.cv1, n2}},
+      {"cv2", {D.cv2, n2}},   {"graphihx", {D.graphihx, n2}}, {"graphihy", {D.graphihy, n2}},
+      {"sch_r", {D.sch_r, n2}}, {"sch_w", {D.sch_w, n2}}, {"bnd_taux", {D.taux, n2}}, {"bnd_tauy", {D.tauy, n2}},
+      {"bnd_t", {D.bnd_t, n2}}, {"bnd_s", {D.bnd_s, n2}}, {"bnd_pa", {D.bnd_pa, n2}}};
+  auto it2 = m2.find(s);
+  if (it2 != m2.end()) return it2->second;
+  // 3-D fields: FP64, or FP32 on the mixed path
+  struct E {
+    const void *p;
+    long long n;
+    int kind, per;
+  };
+  auto table = [&](const auto &X) {
+    return std::map<std::string, E>{
+        {"tc", {X.tc, n3, 0, 1}},     {"sc", {X.sc, n3, 0, 1}},     {"tp", {X.tp, n3, 0, 1}},
+        {"sp", {X.sp, n3, 0, 1}},     {"uc", {X.uc, n3, 0, 1}},     {"vc", {X.vc, n3, 0, 1}},
+        {"up", {X.up, n3, 0, 1}},     {"vp", {X.vp, n3, 0, 1}},     {"auc", {X.auc, n3, 0, 1}},
+        {"aup", {X.aup, n3, 0, 1}},   {"aupp", {X.aupp, n3, 0, 1}}, {"avc", {X.avc, n3, 0, 1}},
+        {"avp", {X.avp, n3, 0, 1}},   {"avpp", {X.avpp, n3, 0, 1}}, {"am", {X.am, n3, 0, 1}},
+        {"alpha", {X.alpha, n3, 1, 1}}, {"adp", {X.adp, n3, 2, 1}}, {"wm", {X.wm, n3p, 0, 1}},
+        {"prho", {X.prho, 2 * n3, 0, 2}}, {"fx", {X.fx, n3, 0, 1}}, {"fy", {X.fy, n3, 0, 1}},
+        {"act", {X.act, n3, 0, 1}},   {"acs", {X.acs, n3, 0, 1}},   {"acr", {X.acr, n3, 0, 1}},
+        {"acu", {X.acu, n3, 0, 1}},   {"acv", {X.acv, n3, 0, 1}},   {"acw", {X.acw, n3, 0, 1}},
+        {"km", {X.km, n3p, 0, 1}},    {"kh", {X.kh, n3p, 0, 1}},    {"uu", {X.uu, n3, 0, 1}},
+        {"vv", {X.vv, n3, 0, 1}}};
+  };
+  if (h->mixed) {
+    auto m3 = table(h->DM);
+    auto it = m3.find(s);
+    if (it == m3.end()) return {nullptr, 0};
+    Named r{nullptr, it->second.n};
+    r.pf = (const float *)it->second.p;
+    r.kind = it->second.kind;
+    r.per = it->second.per;
+    return r;
+  }
+  auto m3 = table(D);
+  auto it = m3.find(s);
+  if (it == m3.end()) return {nullptr, 0};
+  return {(const double *)it->second.p, it->second.n};
+}
+
+// copy a named array to the host as FP64
+int fetch(pcom_handle *h, const char *name, double *dst) {
+  if (!dst) return PCOM_OK;
+  Named f = lookup(h, name);
+  if (f.p) return copy_out(h, dst, f.p, f.n);
+  if (!f.pf) return fail(PCOM_ERR_ARG, "unknown field '%s'", name);
+  return get_f32(h, dst, f.pf, f.n, f.kind, f.per);
+}
+
+}  // namespace
+
+namespace {
+
+// mixed path: fix the reference profile of the alpha/adp anomalies from the
+// level means of T and S over wet points, and re-express stored anomalies
+int set_reference_profile(pcom_handle *h, const double *tc, const double *sc) {
+  const int nk = h->nk;
+  const long long n2 = h->n2;
+  std::vector<double> tr(PCOM_MAXK, 0.0), sr(PCOM_MAXK, 0.0), pr(PCOM_MAXK, 0.0), al(PCOM_MAXK, 0.0);
+  for (int k = 1; k <= nk; ++k) {
+    double st = 0.0, ss = 0.0;
+    long long c = 0;
+    for (long long q = 0; q < n2; ++q) {
+      const bool wet = h->lev_t_host.empty() ? true : h->lev_t_host[q] >= k;
+      if (!wet) continue;
+      st += tc[q + n2 * (k - 1)];
+      ss += sc[q + n2 * (k - 1)];
+      ++c;
+    }
+    tr[k] = c ? st / c : (k > 1 ? tr[k - 1] : 10.0);
+    sr[k] = c ? ss / c : (k > 1 ? sr[k - 1] : 35.0);
+    pr[k] = h->D.pr2[k];
+  }
+  double *d = h->stage;
+  CK(cudaMemcpyAsync(d, tr.data(), PCOM_MAXK * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d + PCOM_MAXK, sr.data(), PCOM_MAXK * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d + 2 * PCOM_MAXK, pr.data(), PCOM_MAXK * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_ref_profile<<<1, 32, 0, h->stream>>>(h->D.c, d, d + PCOM_MAXK, d + 2 * PCOM_MAXK, nk, d + 3 * PCOM_MAXK);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(al.data(), d + 3 * PCOM_MAXK, PCOM_MAXK * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  // stored anomalies were relative to the old profile: re-express them
+  Dev &D = h->D;
+  const Profile old_pr = profile_of(D);
+  for (int k = 1; k <= nk; ++k) D.alpha_r[k] = al[k];
+  D.adp_cum[nk + 1] = 0.0;
+  for (int k = nk; k >= 1; --k) D.adp_cum[k] = D.adp_cum[k + 1] + D.alpha_r[k] * D.dpr2[k];
+  const Profile new_pr = profile_of(D);
+  const long long n3 = h->n3;
+  for (int f = 1; f <= 2; ++f) {
+    float *p = f == 1 ? h->DM.alpha : h->DM.adp;
+    k_to_f64<<<592, 256, 0, h->stream>>>(p, h->stage, n3, n2, 1, f, old_pr);
+    k_to_f32<<<592, 256, 0, h->stream>>>(h->stage, p, n3, n2, 1, f, new_pr);
+    CK(cudaGetLastError());
+  }
+  sync_common(h);
+  h->ref_set = true;
+  CK(cudaStreamSynchronize(h->stream));
+  return PCOM_OK;
+}
+
+int set_state_mixed(pcom_handle *h, const pcom_state *s) {
+  const long long n2 = h->n2, n3 = h->n3, n3p = h->n3p;
+  Dev &D = h->D;
+  DevM &M = h->DM;
+  int rc = 0;
+  if (!h->ref_set && s->tc && s->sc) rc = set_reference_profile(h, s->tc, s->sc);
+  auto in2 = [&](double *dst, const double *src) { if (!rc) rc = copy_in(h, dst, src, n2); };
+  auto in3 = [&](float *dst, const double *src, long long n, int kind, const double *, int per) {
+    if (!rc && src) rc = put_f32(h, dst, src, n, kind, per);
+  };
+  in3(M.tc, s->tc, n3, 0, nullptr, 1); in3(M.sc, s->sc, n3, 0, nullptr, 1);
+  in3(M.tp, s->tp, n3, 0, nullptr, 1); in3(M.sp, s->sp, n3, 0, nullptr, 1);
+  in3(M.uc, s->uc, n3, 0, nullptr, 1); in3(M.vc, s->vc, n3, 0, nullptr, 1);
+  in3(M.up, s->up, n3, 0, nullptr, 1); in3(M.vp, s->vp, n3, 0, nullptr, 1);
+  in3(M.auc, s->auc, n3, 0, nullptr, 1); in3(M.aup, s->aup, n3, 0, nullptr, 1); in3(M.aupp, s->aupp, n3, 0, nullptr, 1);
+  in3(M.avc, s->avc, n3, 0, nullptr, 1); in3(M.avp, s->avp, n3, 0, nullptr, 1); in3(M.avpp, s->avpp, n3, 0, nullptr, 1);
+  in2(D.ubc, s->ubc); in2(D.vbc, s->vbc); in2(D.ubp, s->ubp); in2(D.vbp, s->vbp);
+  in2(D.chc, s->chc); in2(D.chp, s->chp); in2(D.mch, s->mch); in2(D.mch2, s->mch2);
+  in3(M.am, s->am, n3, 0, nullptr, 1);
+  if (!rc && s->am) rc = copy_in(h, D.am1, s->am, n2);
+  in3((float *)M.prho, s->prho, 2 * n3, 0, nullptr, 2);
+  in3(M.alpha, s->alpha, n3, 1, nullptr, 1);
+  in3(M.adp, s->adp, n3, 2, nullptr, 1);
+  in3(M.wm, s->wm, n3p, 0, nullptr, 1);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return PCOM_OK;
 }
 
 }  // namespace
@@ -437,8 +713,8 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   if (d.nk > PCOM_MAXK - 1) return fail(PCOM_ERR_ARG, "nk = %d exceeds the supported %d levels", d.nk, PCOM_MAXK - 1);
   if (d.ni != d.glo_ni + 2 || d.nj != d.glo_nj + 2) return fail(PCOM_ERR_ARG, "ni, nj must be glo_ni + 2, glo_nj + 2");
   if (d.dtbt <= 0 || d.dtbc <= 0 || d.dtbc % d.dtbt != 0) return fail(PCOM_ERR_ARG, "dtbc must be a positive multiple of dtbt");
-  if ((d.flags & PCOM_PREC_MIXED) != 0) return fail(PCOM_ERR_ARG, "mixed precision is not built into this handle type");
   pcom_handle *h = new pcom_handle();
+  h->mixed = (d.flags & PCOM_PREC_MIXED) != 0;
   h->dims = d;
   h->ni = d.ni; h->nj = d.nj; h->nk = d.nk; h->nkp = d.nk + 1;
   h->n2 = (long long)d.ni * d.nj;
@@ -487,25 +763,25 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   A(&p, n2); D.prh_t = p; A(&p, n2); D.phih_t = p; A(&p, n2); D.prh_u = p;
   A(&p, n2); D.cv1 = p; A(&p, n2); D.cv2 = p; A(&p, n2); D.cor = p;
   A(&p, n2); D.graphihx = p; A(&p, n2); D.graphihy = p;
-  A(&p, n3p); D.km = p; A(&p, n3p); D.kh = p;
   A(&p, n2); D.taux = p; A(&p, n2); D.tauy = p; A(&p, n2); D.bnd_t = p; A(&p, n2); D.bnd_s = p; A(&p, n2); D.bnd_pa = p;
-  for (int q = 0; q < 3; ++q) { A(&h->t_pool[q], n3); A(&h->s_pool[q], n3); A(&h->ab_u[q], n3); A(&h->ab_v[q], n3); }
-  A(&D.uc, n3); A(&D.vc, n3); A(&D.up, n3); A(&D.vp, n3);
+  if (!rc) {
+    if (h->mixed) rc = alloc_3d(h, h->DM, h->ab_uf, h->ab_vf, h->t_poolf, h->s_poolf);
+    else rc = alloc_3d(h, D, h->ab_u, h->ab_v, h->t_pool, h->s_pool);
+  }
   A(&D.ubc, n2); A(&D.vbc, n2); A(&D.ubp, n2); A(&D.vbp, n2);
   A(&D.chc, n2); A(&D.chp, n2); A(&D.mch, n2); A(&D.mch2, n2);
-  A(&D.am, n3); A(&D.alpha, n3); A(&D.adp, n3); A(&D.wm, n3p);
-  {
-    double2 *pr = nullptr;
-    if (!rc) rc = h->alloc(&pr, (size_t)n3);
-    D.prho = pr;
-  }
-  A(&D.fx, n3); A(&D.fy, n3); A(&D.pax, n2); A(&D.pay, n2); A(&D.ut, n2); A(&D.vt, n2);
+  A(&D.pax, n2); A(&D.pay, n2); A(&D.ut, n2); A(&D.vt, n2);
   for (int q = 0; q < 4; ++q) { A(&D.bphi[q], n2); A(&D.bgra[q], n2); }
-  A(&D.sch_r, n2); A(&D.sch_w, n2); A(&D.uu, n3); A(&D.vv, n3);
-  A(&D.act, n3); A(&D.acs, n3); A(&D.acr, n3); A(&D.acu, n3); A(&D.acv, n3); A(&D.acw, n3);
+  A(&D.sch_r, n2); A(&D.sch_w, n2);
   A(&D.acch, n2); A(&D.acssh, n2);
   for (int q = 0; q < 2; ++q) { A(&D.tr_ch[q], n2); A(&D.tr_ub[q], n2); A(&D.tr_vb[q], n2); }
   for (int q = 0; q < 6; ++q) A(&D.tr_acc[q], n2);
+  A(&D.am1, n2);
+  if (h->mixed) {
+    D.am = D.am1;  // the barotropic kernel reads am at level 1 only
+    A(&h->stage, std::max(n3p, 2 * n3));
+  }
+  A(&h->d_sums, 3 * 1024 + 3);
   unsigned *bar = nullptr;
   int *err = nullptr;
   if (!rc) rc = h->alloc(&bar, 4);
@@ -522,14 +798,25 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   {
     LitMode lit{(d.flags & PCOM_LIT_R8) != 0};
     std::vector<double> v((size_t)n3, lit(1.0f / 1000.0f, 1.0 / 1000.0));
-    cudaMemcpy(D.alpha, v.data(), n3 * sizeof(double), cudaMemcpyHostToDevice);
-    std::fill(v.begin(), v.end(), LIT(1.0e3));
-    cudaMemcpy(D.am, v.data(), n3 * sizeof(double), cudaMemcpyHostToDevice);
+    if (h->mixed) {
+      // the anomaly profile is zero until the first state arrives
+      std::vector<float> f((size_t)n3, (float)v[0]);
+      cudaMemcpy(h->DM.alpha, f.data(), n3 * sizeof(float), cudaMemcpyHostToDevice);
+      std::fill(f.begin(), f.end(), (float)LIT(1.0e3));
+      cudaMemcpy(h->DM.am, f.data(), n3 * sizeof(float), cudaMemcpyHostToDevice);
+      std::fill(v.begin(), v.end(), LIT(1.0e3));
+      cudaMemcpy(D.am1, v.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    } else {
+      cudaMemcpy(D.alpha, v.data(), n3 * sizeof(double), cudaMemcpyHostToDevice);
+      std::fill(v.begin(), v.end(), LIT(1.0e3));
+      cudaMemcpy(D.am, v.data(), n3 * sizeof(double), cudaMemcpyHostToDevice);
+    }
     std::vector<double> one((size_t)n2, 1.0);
     for (double *c : {D.chc, D.chp, D.mch, D.mch2}) cudaMemcpy(c, one.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
   }
   h->itc = h->itp = 0;
   h->ic = 0; h->ip = 1; h->ipp = 2;
+  sync_common(h);
   bind_rotating(h);
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) { pcom_gpu_destroy(h); return fail(PCOM_ERR_CUDA, "init: %s", cudaGetErrorString(e)); }
@@ -657,12 +944,22 @@ int pcom_gpu_upload_static(pcom_handle *h, const pcom_static *s) {
     CK(cudaMemcpy((void *)dst2[q], src2[q], n2 * sizeof(double), cudaMemcpyHostToDevice));
   }
   if (!s->km || !s->kh) return fail(PCOM_ERR_ARG, "km/kh missing");
-  CK(cudaMemcpy((void *)D.km, s->km, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy((void *)D.kh, s->kh, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
+  if (h->mixed) {
+    int rc2 = put_f32(h, (float *)h->DM.km, s->km, h->n3p, 0);
+    if (!rc2) rc2 = put_f32(h, (float *)h->DM.kh, s->kh, h->n3p, 0);
+    if (rc2) return rc2;
+    CK(cudaStreamSynchronize(h->stream));
+  } else {
+    CK(cudaMemcpy((void *)D.km, s->km, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void *)D.kh, s->kh, h->n3p * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  h->lev_t_host.assign(s->lev_t, s->lev_t + n2);
   if (!s->pr2 || !s->dpr2 || !s->dz1) return fail(PCOM_ERR_ARG, "vertical grid missing");
   for (int k = 1; k <= nk; ++k) { D.pr2[k] = s->pr2[k - 1]; D.dpr2[k] = s->dpr2[k - 1]; D.rdpr2[k] = 1.0 / s->dpr2[k - 1]; }
   for (int k = 1; k <= nkp; ++k) { D.dz1[k] = s->dz1[k - 1]; D.rdz1[k] = 1.0 / s->dz1[k - 1]; }
+  for (int k = 1; k <= nk; ++k) D.dz2[k] = s->dz2 ? s->dz2[k - 1] : 0.0;
   (void)ni; (void)nj;
+  sync_common(h);
   h->static_ok = true;
   return PCOM_OK;
 }
@@ -677,12 +974,18 @@ int pcom_gpu_set_state(pcom_handle *h, const pcom_state *s) {
       int fr = 0;
       while (fr == h->itc) ++fr;
       // preserve the current tc/sc contents in the new tp buffer first
-      CK(cudaMemcpyAsync(h->t_pool[fr], h->t_pool[h->itc], n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-      CK(cudaMemcpyAsync(h->s_pool[fr], h->s_pool[h->itc], n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      if (h->mixed) {
+        CK(cudaMemcpyAsync(h->t_poolf[fr], h->t_poolf[h->itc], n3 * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->s_poolf[fr], h->s_poolf[h->itc], n3 * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+      } else {
+        CK(cudaMemcpyAsync(h->t_pool[fr], h->t_pool[h->itc], n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->s_pool[fr], h->s_pool[h->itc], n3 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      }
       h->itp = fr;
       bind_rotating(h);
     }
   }
+  if (h->mixed) return set_state_mixed(h, s);
   int rc = 0;
   auto in = [&](double *dst, const double *src, long long n) { if (!rc) rc = copy_in(h, dst, src, n); };
   in(D.tc, s->tc, n3); in(D.sc, s->sc, n3); in(D.tp, s->tp, n3); in(D.sp, s->sp, n3);
@@ -700,18 +1003,16 @@ int pcom_gpu_set_state(pcom_handle *h, const pcom_state *s) {
 
 int pcom_gpu_get_state(pcom_handle *h, pcom_state *s) {
   if (!h || !s) return fail(PCOM_ERR_ARG, "null argument");
-  const long long n2 = h->n2, n3 = h->n3;
-  Dev &D = h->D;
   int rc = 0;
-  auto out = [&](double *dst, const double *src, long long n) { if (!rc) rc = copy_out(h, dst, src, n); };
-  out(s->tc, D.tc, n3); out(s->sc, D.sc, n3); out(s->tp, D.tp, n3); out(s->sp, D.sp, n3);
-  out(s->uc, D.uc, n3); out(s->vc, D.vc, n3); out(s->up, D.up, n3); out(s->vp, D.vp, n3);
-  out(s->auc, D.auc, n3); out(s->aup, D.aup, n3); out(s->aupp, D.aupp, n3);
-  out(s->avc, D.avc, n3); out(s->avp, D.avp, n3); out(s->avpp, D.avpp, n3);
-  out(s->ubc, D.ubc, n2); out(s->vbc, D.vbc, n2); out(s->ubp, D.ubp, n2); out(s->vbp, D.vbp, n2);
-  out(s->chc, D.chc, n2); out(s->chp, D.chp, n2); out(s->mch, D.mch, n2); out(s->mch2, D.mch2, n2);
-  out(s->am, D.am, n3); out(s->prho, (const double *)D.prho, 2 * n3);
-  out(s->alpha, D.alpha, n3); out(s->adp, D.adp, n3); out(s->wm, D.wm, h->n3p);
+  auto out = [&](double *dst, const char *name) { if (!rc) rc = fetch(h, name, dst); };
+  out(s->tc, "tc"); out(s->sc, "sc"); out(s->tp, "tp"); out(s->sp, "sp");
+  out(s->uc, "uc"); out(s->vc, "vc"); out(s->up, "up"); out(s->vp, "vp");
+  out(s->auc, "auc"); out(s->aup, "aup"); out(s->aupp, "aupp");
+  out(s->avc, "avc"); out(s->avp, "avp"); out(s->avpp, "avpp");
+  out(s->ubc, "ubc"); out(s->vbc, "vbc"); out(s->ubp, "ubp"); out(s->vbp, "vbp");
+  out(s->chc, "chc"); out(s->chp, "chp"); out(s->mch, "mch"); out(s->mch2, "mch2");
+  out(s->am, "am"); out(s->prho, "prho");
+  out(s->alpha, "alpha"); out(s->adp, "adp"); out(s->wm, "wm");
   if (rc) return rc;
   return sync_check(h);
 }
@@ -728,13 +1029,11 @@ int pcom_gpu_set_forcing(pcom_handle *h, const pcom_forcing *f) {
 
 int pcom_gpu_get_accum(pcom_handle *h, pcom_accum *a) {
   if (!h || !a) return fail(PCOM_ERR_ARG, "null argument");
-  const long long n2 = h->n2, n3 = h->n3;
-  Dev &D = h->D;
   int rc = 0;
-  auto out = [&](double *dst, const double *src, long long n) { if (!rc) rc = copy_out(h, dst, src, n); };
-  out(a->act, D.act, n3); out(a->acs, D.acs, n3); out(a->acr, D.acr, n3);
-  out(a->acu, D.acu, n3); out(a->acv, D.acv, n3); out(a->acw, D.acw, n3);
-  out(a->acch, D.acch, n2); out(a->acssh, D.acssh, n2);
+  auto out = [&](double *dst, const char *name) { if (!rc) rc = fetch(h, name, dst); };
+  out(a->act, "act"); out(a->acs, "acs"); out(a->acr, "acr");
+  out(a->acu, "acu"); out(a->acv, "acv"); out(a->acw, "acw");
+  out(a->acch, "acch"); out(a->acssh, "acssh");
   a->n_ts = h->n_ts; a->n_uv = h->n_uv; a->n_w = h->n_w; a->n_ch = h->n_ch; a->n_ssh = h->n_ssh;
   if (rc) return rc;
   return sync_check(h);
@@ -743,8 +1042,13 @@ int pcom_gpu_get_accum(pcom_handle *h, pcom_accum *a) {
 int pcom_gpu_reset_accum(pcom_handle *h) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   Dev &D = h->D;
-  for (double *p : {D.act, D.acs, D.acr, D.acu, D.acv, D.acw})
-    CK(cudaMemsetAsync(p, 0, h->n3 * sizeof(double), h->stream));
+  if (h->mixed) {
+    for (float *p : {h->DM.act, h->DM.acs, h->DM.acr, h->DM.acu, h->DM.acv, h->DM.acw})
+      CK(cudaMemsetAsync(p, 0, h->n3 * sizeof(float), h->stream));
+  } else {
+    for (double *p : {D.act, D.acs, D.acr, D.acu, D.acv, D.acw})
+      CK(cudaMemsetAsync(p, 0, h->n3 * sizeof(double), h->stream));
+  }
   for (double *p : {D.acch, D.acssh}) CK(cudaMemsetAsync(p, 0, h->n2 * sizeof(double), h->stream));
   h->n_ts = h->n_uv = h->n_w = h->n_ch = h->n_ssh = 0;
   return sync_check(h);
@@ -755,7 +1059,8 @@ int pcom_gpu_den_prho(pcom_handle *h) {
   if (!h->static_ok) return fail(PCOM_ERR_STATE, "den_prho before pcom_gpu_upload_static");
   {
     Prof p(h, "den_prho");
-    launch_den_prho(h->D, h->stream);
+    if (h->mixed) launch_den_prho(h->DM, h->stream);
+    else launch_den_prho(h->D, h->stream);
   }
   return sync_check(h);
 }
@@ -784,9 +1089,10 @@ int64_t pcom_gpu_field_size(pcom_handle *h, const char *name) {
 int pcom_gpu_get_field(pcom_handle *h, const char *name, double *host, int64_t n) {
   if (!h || !name || !host) return fail(PCOM_ERR_ARG, "null argument");
   Named f = lookup(h, name);
-  if (!f.p) return fail(PCOM_ERR_ARG, "unknown field '%s'", name);
+  if (!f.p && !f.pf) return fail(PCOM_ERR_ARG, "unknown field '%s'", name);
   if (n < f.n) return fail(PCOM_ERR_ARG, "buffer for '%s' holds %lld < %lld doubles", name, (long long)n, f.n);
-  CK(cudaMemcpyAsync(host, f.p, f.n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  int rc = fetch(h, name, host);
+  if (rc) return rc;
   return sync_check(h);
 }
 
@@ -794,12 +1100,24 @@ int pcom_gpu_check_finite(pcom_handle *h) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   Dev &D = h->D;
   CK(cudaMemsetAsync(h->d_count, 0, sizeof(unsigned long long), h->stream));
-  struct F { const double *p; const int *lev; int planes; } fs[] = {
-      {D.tc, D.lev_t, h->nk}, {D.sc, D.lev_t, h->nk}, {D.uc, D.lev_u, h->nk}, {D.vc, D.lev_u, h->nk},
-      {D.chc, D.lev_t, 1},    {D.ubc, D.lev_u, 1},    {D.vbc, D.lev_u, 1}};
-  for (auto &f : fs) {
+  if (h->mixed) {
+    const DevM &M = h->DM;
+    struct F { const float *p; const int *lev; } fs[] = {{M.tc, D.lev_t}, {M.sc, D.lev_t}, {M.uc, D.lev_u}, {M.vc, D.lev_u}};
+    for (auto &f : fs) {
+      Prof p(h, "watchdog");
+      k_nonfinite<float><<<592, 256, 0, h->stream>>>(f.p, f.lev, h->nk, h->n2, h->nk, h->d_count);
+    }
+  } else {
+    struct F { const double *p; const int *lev; } fs[] = {{D.tc, D.lev_t}, {D.sc, D.lev_t}, {D.uc, D.lev_u}, {D.vc, D.lev_u}};
+    for (auto &f : fs) {
+      Prof p(h, "watchdog");
+      launch_nonfinite(f.p, f.lev, h->nk, h->n2, h->nk, h->d_count, h->stream);
+    }
+  }
+  struct G { const double *p; const int *lev; } gs[] = {{D.chc, D.lev_t}, {D.ubc, D.lev_u}, {D.vbc, D.lev_u}};
+  for (auto &f : gs) {
     Prof p(h, "watchdog");
-    launch_nonfinite(f.p, f.lev, h->nk, h->n2, f.planes, h->d_count, h->stream);
+    launch_nonfinite(f.p, f.lev, h->nk, h->n2, 1, h->d_count, h->stream);
   }
   unsigned long long c = 0;
   CK(cudaMemcpyAsync(&c, h->d_count, sizeof c, cudaMemcpyDeviceToHost, h->stream));
@@ -807,6 +1125,19 @@ int pcom_gpu_check_finite(pcom_handle *h) {
   if (rc) return rc;
   if (c) return fail(PCOM_ERR_NUMERIC, "%llu non-finite wet values in the prognostic fields", c);
   return PCOM_OK;
+}
+
+int pcom_gpu_global_sums(pcom_handle *h, double *out3) {
+  if (!h || !out3) return fail(PCOM_ERR_ARG, "null argument");
+  if (!h->static_ok) return fail(PCOM_ERR_STATE, "global sums before pcom_gpu_upload_static");
+  const int nb = 1024;
+  if (h->mixed) k_sums<float><<<nb, 256, 0, h->stream>>>(h->DM, h->d_sums);
+  else k_sums<double><<<nb, 256, 0, h->stream>>>(h->D, h->d_sums);
+  k_sums_final<<<1, 32, 0, h->stream>>>(h->d_sums, nb, h->d_sums + 3 * nb);
+  CK(cudaGetLastError());
+  h->launches += 2;
+  CK(cudaMemcpyAsync(out3, h->d_sums + 3 * nb, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return sync_check(h);
 }
 
 int pcom_gpu_set_stream(pcom_handle *h, void *stream) {
@@ -1079,6 +1410,7 @@ int pcom_gpu_batch_create(pcom_handle *const *hs, int32_t n, pcom_batch **out) {
     pcom_handle *h = hs[m];
     if (!h || !h->static_ok) { delete b; return fail(PCOM_ERR_STATE, "batch member %d has no static data", m); }
     if (!h->D.separable) { delete b; return fail(PCOM_ERR_ARG, "batch member %d: batches need lat-lon (separable) metrics", m); }
+    if (h->mixed) { delete b; return fail(PCOM_ERR_ARG, "batch member %d: batches run the FP64 path only", m); }
     if (h->D.bt != hs[0]->D.bt || h->D.bc != hs[0]->D.bc) { delete b; return fail(PCOM_ERR_ARG, "batch members must share dtbt and dtbc"); }
     if (h->device != hs[0]->device) { delete b; return fail(PCOM_ERR_ARG, "batch members must live on one device"); }
     b->hs.push_back(h);

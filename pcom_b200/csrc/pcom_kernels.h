@@ -3,16 +3,26 @@
 #include <cuda_runtime.h>
 #include "pcom_dev.cuh"
 
-void launch_alpha_tobot(const Dev &P, cudaStream_t s);
-void launch_pgra2d(const Dev &P, cudaStream_t s);
-void launch_uv2d(const Dev &P, int mode, cudaStream_t s);
-void launch_upwelling(const Dev &P, int with_acw, cudaStream_t s);
-void launch_readyc3d(const Dev &P, cudaStream_t s);
-void launch_clin(const Dev &P, cudaStream_t s);
-void launch_smag(const Dev &P, cudaStream_t s);
-void launch_ssh(const Dev &P, cudaStream_t s);
-void launch_ts(const Dev &P, cudaStream_t s);
-void launch_den_prho(const Dev &P, cudaStream_t s);
+template <typename R>
+void launch_alpha_tobot(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_pgra2d(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_uv2d(const DevT<R> &P, int mode, cudaStream_t s);
+template <typename R>
+void launch_upwelling(const DevT<R> &P, int with_acw, cudaStream_t s);
+template <typename R>
+void launch_readyc3d(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_clin(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_smag(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_ssh(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_ts(const DevT<R> &P, cudaStream_t s);
+template <typename R>
+void launch_den_prho(const DevT<R> &P, cudaStream_t s);
 
 // batched forms: member m = blockIdx.z reads its Dev from dPs[m]
 struct BatchShape {

@@ -183,6 +183,12 @@ class Model:
     def launch_count(self) -> int:
         return int(self.lib.pcom_gpu_launch_count(self.handle))
 
+    def global_sums(self) -> tuple:
+        """(volume m^3, sum T dV, sum S dV) over the wet interior, FP64."""
+        out = np.zeros(3)
+        L.check(self.lib.pcom_gpu_global_sums(self.handle, _dp(out)), "global_sums")
+        return tuple(float(x) for x in out)
+
 
 class Batch:
     """Several models stepped together on one device (ensemble members and
