@@ -112,6 +112,25 @@ SIGNATURES = {
     "pcom_gpu_batch_launch_count": (C.c_int64, [C.c_void_p]),
     "pcom_gpu_batch_use_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    # closure network (include/pcom_cnn.h)
+    "pcom_cnn_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
+    "pcom_cnn_param_count": (C.c_int64, []),
+    "pcom_cnn_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "pcom_cnn_destroy": (C.c_int, [C.c_void_p]),
+    "pcom_cnn_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pcom_cnn_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "pcom_cnn_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "pcom_cnn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "pcom_cnn_forward_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "pcom_cnn_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                    C.POINTER(C.c_double)]),
+    "pcom_cnn_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float,
+                                      C.POINTER(C.c_double)]),
+    "pcom_cnn_conv_layer": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_void_p]),
+    "pcom_cnn_wgrad_layer": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "pcom_model_create": (C.c_int, [C.POINTER(Case), C.c_int32, C.POINTER(C.c_void_p)]),
     "pcom_model_destroy": (C.c_int, [C.c_void_p]),
     "pcom_model_handle": (C.c_void_p, [C.c_void_p]),

@@ -18,7 +18,7 @@ LIB = os.path.join(OUT_DIR, "libpcomgpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FP64 = ["k_step.cu", "k_trop.cu", "pcom_gpu.cu", "k_trop_noalloc.cu", "k_trop_batch.cu"]
-CU_FAST = []  # kernels allowed to contract a*b+c into FMA (mixed precision)
+CU_FAST = ["k_cnn.cu", "cnn.cu"]  # kernels allowed to contract a*b+c into FMA (the closure network)
 CPP = ["pcom_host.cpp"]
 
 
@@ -37,7 +37,7 @@ def _host_cxx() -> str:
 def _sources():
     return [os.path.join(SRC, f) for f in CU_FP64 + CU_FAST + CPP] + [
         os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".cuh", ".h"))
-    ] + [os.path.join(HERE, "..", "include", f) for f in ("pcom_gpu.h", "pcom_host.h")]
+    ] + [os.path.join(HERE, "..", "include", f) for f in ("pcom_gpu.h", "pcom_host.h", "pcom_cnn.h")]
 
 
 def up_to_date() -> bool:

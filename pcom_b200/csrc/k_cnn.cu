@@ -1,0 +1,412 @@
+// k_cnn.cu -- the learned subgrid closure: a 5-layer 3x3 convolutional
+// network (input channels u, v, T, S and the specific-volume anomaly per
+// model level; 64 hidden channels; outputs the du, dv, dT, dS tendency
+// residuals), trained and evaluated with the kernels below.
+//
+// Every convolution is an implicit GEMM on the 5th-generation tensor cores:
+// BF16 operands staged in shared memory in the UMMA "interleave" (no
+// swizzle) canonical layout, one elected thread issuing tcgen05.mma
+// (kind::f16, FP32 accumulation in tensor memory), completion tracked with
+// tcgen05.commit on an mbarrier, and the epilogue reading the accumulator
+// with tcgen05.ld.  Forward and data-gradient convolutions are K-major GEMMs
+// (rows = pixels, K = tap x input channel, N = output channels); the weight
+// gradient is an MN-major GEMM (rows = tap x input channel, N = output
+// channels, K = pixels) split over CTAs with FP32 atomics.
+//
+// Activations are NHWC over images of H x W pixels (one image per model
+// level), channels contiguous: 16 (the 5 inputs, zero-padded) or 64.
+// Weights are [9 taps][N out][K in] (K contiguous).  Halo: zero padding in
+// y and, when periodic_x, wrap-around in x (the zonally periodic grid).
+//
+// Every wait is bounded: a timed-out mbarrier wait sets the error flag,
+// waits (bounded) once more for the MMAs in flight, frees tensor memory and
+// returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cnn_kernels.h"
+
+namespace {
+
+constexpr long long kSpin = 1LL << 22;  // try_wait suspends in hardware between polls
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory matrix descriptor, no swizzle: start address, leading
+// (K-direction core-matrix) byte offset, stride (M/N-direction 8-row group)
+// byte offset, each without their 4 low bits; version 1 at bit 46.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor for kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
+// (bits 7-9 = 1, 10-12 = 1), A/B major (bit 15/16: 0 = K, 1 = MN),
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+
+// bounded wait for phase `parity` of an mbarrier
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+  const int n = valid ? 16 : 0;  // 0: zero-fill
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(ncols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// source pixel of tap t (0..8, dy = t/3 - 1, dx = t%3 - 1) for pixel p; -1 if padding
+__device__ __forceinline__ long long tap_src(long long p, int t, int H, int W, int periodic_x) {
+  const long long hw = (long long)H * W;
+  const long long img = p / hw;
+  const int rem = (int)(p - img * hw);
+  int y = rem / W + (t / 3 - 1), x = rem % W + (t % 3 - 1);
+  if (y < 0 || y >= H) return -1;
+  if (x < 0 || x >= W) {
+    if (!periodic_x) return -1;
+    x = (x + W) % W;
+  }
+  return img * hw + (long long)y * W + x;
+}
+
+constexpr int kThreads = 128;  // 4 warps: one TMEM lane quarter each
+constexpr int kM = 128;        // pixels (fwd/dgrad) or tap x channel rows (wgrad) per tile
+
+// ----------------------------------------------------------------------------
+// Forward / data-gradient convolution: out[p][n] = sum_t sum_c in[src(p, t)][c] w[t][n][c]
+// mode 0: + bias, ReLU, BF16 out (stride NOUT)
+// mode 1: + bias, FP32 out, first nstore channels (stride nstore)
+// mode 2: ReLU mask from aux (BF16, stride NOUT): out = acc * (aux > 0), BF16
+template <int CIN, int NOUT>
+__global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__restrict__ in,
+                                                      const __nv_bfloat16 *__restrict__ w,
+                                                      const float *__restrict__ bias, const __nv_bfloat16 *__restrict__ aux,
+                                                      void *out, long long npix, int H, int W, int periodic_x, int mode,
+                                                      int nstore, int *err) {
+  constexpr int KC = CIN / 8;                 // 16-byte chunks per pixel per tap
+  constexpr int A_BYTES = kM * CIN * 2;
+  constexpr int B_BYTES = NOUT * CIN * 2;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const long long p0 = (long long)blockIdx.x * kM;
+
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), NCOLS);
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
+  uint32_t phase[2] = {0, 0};
+  bool ok = true;
+
+  for (int t = 0; t < 9; ++t) {
+    const int s = t & 1;
+    uint8_t *A = smem + s * STAGE, *B = A + A_BYTES;
+    if (t >= 2) {  // the MMAs of tap t-2 read this stage
+      if (!mbar_wait(smem_u32(&mbar[s]), phase[s])) ok = false;
+      phase[s] ^= 1;
+    }
+    // A: 128 pixels x KC chunks, core matrix (g, c) at ((g*KC + c) * 128) + (m%8)*16
+    for (int q = tid; q < kM * KC; q += kThreads) {
+      const int m = q / KC, c = q % KC;
+      const long long p = p0 + m;
+      const long long src = p < npix ? tap_src(p, t, H, W, periodic_x) : -1;
+      const uint32_t dst = smem_u32(A) + (uint32_t)(((m / 8) * KC + c) * 128 + (m % 8) * 16);
+      cp_async16(dst, src >= 0 ? (const void *)(in + src * CIN + c * 8) : (const void *)in, src >= 0);
+    }
+    // B: NOUT rows x KC chunks of tap t
+    for (int q = tid; q < NOUT * KC; q += kThreads) {
+      const int n = q / KC, c = q % KC;
+      const uint32_t dst = smem_u32(B) + (uint32_t)(((n / 8) * KC + c) * 128 + (n % 8) * 16);
+      cp_async16(dst, w + ((long long)t * NOUT + n) * CIN + c * 8, true);
+    }
+    cp_async_wait_all();
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0 && ok) {
+      tc_fence_after();
+      #pragma unroll
+      for (int j = 0; j < CIN / 16; ++j) {
+        const uint64_t ad = umma_desc(smem_u32(A) + j * 256, 128, KC * 128);
+        const uint64_t bd = umma_desc(smem_u32(B) + j * 256, 128, KC * 128);
+        umma_bf16(tmem, ad, bd, idesc, (t > 0 || j > 0) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&mbar[s]));
+    }
+    __syncthreads();
+  }
+  // the last commit (tap 8, stage 0) covers every MMA issued before it
+  if (!mbar_wait(smem_u32(&mbar[0]), phase[0])) ok = false;
+  if (!mbar_wait(smem_u32(&mbar[1]), phase[1])) ok = false;
+  tc_fence_after();
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    const int row = warp * 32 + lane;
+    const long long p = p0 + row;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    #pragma unroll
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      float v[16];
+      tmem_ld16(lane_addr + c0, v);
+      if (p < npix) {
+        if (mode == 0) {
+          __nv_bfloat16 *o = (__nv_bfloat16 *)out + p * NOUT + c0;
+          #pragma unroll
+          for (int q = 0; q < 16; ++q) o[q] = __float2bfloat16(fmaxf(v[q] + bias[c0 + q], 0.f));
+        } else if (mode == 1) {
+          float *o = (float *)out + p * nstore;
+          for (int q = 0; q < 16; ++q)
+            if (c0 + q < nstore) o[c0 + q] = v[q] + bias[c0 + q];
+        } else {
+          __nv_bfloat16 *o = (__nv_bfloat16 *)out + p * NOUT + c0;
+          const __nv_bfloat16 *a = aux + p * NOUT + c0;
+          #pragma unroll
+          for (int q = 0; q < 16; ++q) o[q] = __float2bfloat16(__bfloat162float(a[q]) > 0.f ? v[q] : 0.f);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+}
+
+// ----------------------------------------------------------------------------
+// Weight gradient: dw[t][n][c] += sum_p in[src(p, t)][c] g[p][n]
+// Tile rows r = (t - t0) * CIN + c for TPT = 128 / CIN taps starting at
+// t0 = blockIdx.y * TPT; K = pixels, 64 per stage; CTA x covers ppc pixels.
+template <int CIN, int NOUT>
+__global__ void __launch_bounds__(kThreads) k_wgrad_tc(const __nv_bfloat16 *__restrict__ in,
+                                                       const __nv_bfloat16 *__restrict__ g, float *dw, long long npix,
+                                                       int H, int W, int periodic_x, long long ppc, int *err) {
+  constexpr int TPT = kM / CIN;
+  constexpr int KP = 64;                  // pixels per stage
+  constexpr int KG = KP / 8;              // K groups (8 pixels) per stage
+  constexpr int A_BYTES = kM * KP * 2;    // 128 rows x 64 pixels
+  constexpr int B_BYTES = NOUT * KP * 2;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int t0 = blockIdx.y * TPT;
+  const long long pbeg = (long long)blockIdx.x * ppc;
+  const long long pend = min(npix, pbeg + ppc);
+  const int nstage = (int)((pend - pbeg + KP - 1) / KP);
+
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), NCOLS);
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 1, 1);
+  uint32_t phase[2] = {0, 0};
+  bool ok = true;
+  int issued[2] = {0, 0};
+
+  for (int st = 0; st < nstage; ++st) {
+    const int s = st & 1;
+    uint8_t *A = smem + s * STAGE, *B = A + A_BYTES;
+    if (st >= 2) {
+      if (!mbar_wait(smem_u32(&mbar[s]), phase[s])) ok = false;
+      phase[s] ^= 1;
+    }
+    const long long pk = pbeg + (long long)st * KP;
+    // A (MN-major): core (g, kg) = 8 pixels x 8 channels at (g*KG + kg)*128,
+    // pixel k of the group at k*16; row group g = (tap, channel chunk)
+    for (int q = tid; q < (kM / 8) * KP; q += kThreads) {
+      const int g = q / KP, k = q % KP;
+      const int r0 = g * 8, t = t0 + r0 / CIN, c = r0 % CIN;
+      const long long p = pk + k;
+      const long long src = (t < 9 && p < pend) ? tap_src(p, t, H, W, periodic_x) : -1;
+      const uint32_t dst = smem_u32(A) + (uint32_t)((g * KG + k / 8) * 128 + (k % 8) * 16);
+      cp_async16(dst, src >= 0 ? (const void *)(in + src * CIN + c) : (const void *)in, src >= 0);
+    }
+    // B (MN-major): core (gn, kg) = 8 pixels x 8 output channels
+    for (int q = tid; q < (NOUT / 8) * KP; q += kThreads) {
+      const int gn = q / KP, k = q % KP;
+      const long long p = pk + k;
+      const uint32_t dst = smem_u32(B) + (uint32_t)((gn * KG + k / 8) * 128 + (k % 8) * 16);
+      cp_async16(dst, p < pend ? (const void *)(g + p * NOUT + gn * 8) : (const void *)g, p < pend);
+    }
+    cp_async_wait_all();
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0 && ok) {
+      tc_fence_after();
+      #pragma unroll
+      for (int j = 0; j < KP / 16; ++j) {
+        const uint64_t ad = umma_desc(smem_u32(A) + j * 256, 128, KG * 128);
+        const uint64_t bd = umma_desc(smem_u32(B) + j * 256, 128, KG * 128);
+        umma_bf16(tmem, ad, bd, idesc, (st > 0 || j > 0) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&mbar[s]));
+    }
+    issued[s]++;
+    __syncthreads();
+  }
+  for (int s = 0; s < 2; ++s)
+    if (issued[s] > 0 && nstage > 0) {
+      // stages s, s+2, ...: the outstanding phase of mbar[s] is the last one
+      if (!mbar_wait(smem_u32(&mbar[s]), phase[s])) ok = false;
+    }
+  tc_fence_after();
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else if (nstage > 0) {
+    const int row = warp * 32 + lane;
+    const int t = t0 + row / CIN, c = row % CIN;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    #pragma unroll
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      float v[16];
+      tmem_ld16(lane_addr + c0, v);
+      if (t < 9)
+        for (int q = 0; q < 16; ++q) atomicAdd(dw + ((long long)t * NOUT + c0 + q) * CIN + c, v[q]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+}
+
+// dynamic shared memory per CTA; with 64 accumulator columns at least 29 KB,
+// so that at most 7 CTAs share an SM's 512 tensor-memory columns
+template <int NOUT>
+size_t smem_floor(size_t b) { return NOUT > 32 && b < 29 * 1024 ? 29 * 1024 : b; }
+template <int CIN, int NOUT>
+size_t conv_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * CIN * 2 + NOUT * CIN * 2)); }
+template <int CIN, int NOUT>
+size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 64 * 2)); }
+
+template <int CIN, int NOUT>
+cudaError_t conv_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, const __nv_bfloat16 *aux,
+                        void *out, long long npix, int H, int W, int periodic_x, int mode, int nstore, int *err,
+                        cudaStream_t s) {
+  const size_t sm = conv_smem<CIN, NOUT>();
+  cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)((npix + kM - 1) / kM);
+  k_conv_tc<CIN, NOUT><<<grid, kThreads, sm, s>>>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err);
+  return cudaGetLastError();
+}
+
+template <int CIN, int NOUT>
+cudaError_t wgrad_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, long long npix, int H, int W,
+                         int periodic_x, int *err, cudaStream_t s) {
+  const size_t sm = wgrad_smem<CIN, NOUT>();
+  cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  constexpr int TPT = kM / CIN;
+  const int ytiles = (9 + TPT - 1) / TPT;
+  // split K over about 4 waves of CTAs; pixels per CTA a multiple of 64
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  long long target = (long long)nsm * 8 / ytiles;
+  if (target < 1) target = 1;
+  long long ppc = (npix + target - 1) / target;
+  ppc = (ppc + 63) / 64 * 64;
+  if (ppc < 64) ppc = 64;
+  const unsigned gx = (unsigned)((npix + ppc - 1) / ppc);
+  k_wgrad_tc<CIN, NOUT><<<dim3(gx, ytiles), kThreads, sm, s>>>(in, g, dw, npix, H, W, periodic_x, ppc, err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t cnn_conv(int cin, int nout, const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                     const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x, int mode,
+                     int nstore, int *err, cudaStream_t s) {
+  if (cin == 16 && nout == 64) return conv_launch<16, 64>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+  if (cin == 64 && nout == 64) return conv_launch<64, 64>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+  if (cin == 64 && nout == 16) return conv_launch<64, 16>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+  if (cin == 16 && nout == 16) return conv_launch<16, 16>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t cnn_wgrad(int cin, int nout, const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, long long npix,
+                      int H, int W, int periodic_x, int *err, cudaStream_t s) {
+  if (cin == 16 && nout == 64) return wgrad_launch<16, 64>(in, g, dw, npix, H, W, periodic_x, err, s);
+  if (cin == 64 && nout == 64) return wgrad_launch<64, 64>(in, g, dw, npix, H, W, periodic_x, err, s);
+  if (cin == 64 && nout == 16) return wgrad_launch<64, 16>(in, g, dw, npix, H, W, periodic_x, err, s);
+  return cudaErrorInvalidValue;
+}
