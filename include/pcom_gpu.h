@@ -173,6 +173,35 @@ int pcom_gpu_profile_read(pcom_handle *h, char *names, int64_t *launches, double
 /* Number of this library's kernel launches issued so far on this handle. */
 int64_t pcom_gpu_launch_count(pcom_handle *h);
 
+/* --- closure coupling ----------------------------------------------------- */
+/* No counterpart in the reference.  Data and corrections for the learned
+ * subgrid closure (include/pcom_cnn.h) on FP64 handles. */
+typedef struct {
+  float in_mean[5], in_std[5];  /* u, v, T, S, alpha - alpha_ref(k) */
+  float out_std[4];             /* du, dv, dT, dS tendency scales */
+  double alpha_ref[64];         /* [k - 1], k = 1..nk */
+} pcom_cnn_stats;
+/* Set the coarse handle's state to the block means (factor x factor) of the
+ * fine handle's state over wet fine cells: T-grid fields (tc, sc, tp, sp,
+ * ch, mch, mch2) on T cells, U-grid fields (uc, vc, up, vp, the AB3
+ * history, am, ub, vb) on U points.  The grids must nest: fine glo_ni,
+ * glo_nj = factor x coarse, and the coarse levels no deeper than any fine
+ * column of their block. */
+int pcom_gpu_coarsen(pcom_handle *fine, pcom_handle *coarse, int32_t factor);
+/* Network input from the state: BF16 [nk][glo_nj][glo_ni][16] (device),
+ * channels (uc, vc, tc, sc, alpha - alpha_ref) normalised by `stats`, zero
+ * on land and in channels 5..15. */
+int pcom_gpu_cnn_features(pcom_handle *h, void *x_bf16, const pcom_cnn_stats *stats);
+/* Training target: (truth - pred) / dt / out_std per channel into FP32
+ * [nk][glo_nj][glo_ni][4] (device), and the wet mask (U points for u, v, T
+ * cells for T, S) into `mask` of the same shape (either may be NULL). */
+int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, float *mask, const pcom_cnn_stats *stats,
+                        double dt);
+/* Apply the network's output y (FP32 [nk][glo_nj][glo_ni][4], device) as a
+ * tendency over dt seconds: uc, up += dt out_std[0] y0 (wet U points), vc,
+ * vp likewise, tc, tp, sc, sp on wet T cells. */
+int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *stats, double dt);
+
 /* --- batches -------------------------------------------------------------- */
 /* No counterpart in the reference (it runs one domain per MPI job).  A batch
  * steps several handles together -- ensemble members and basins of uneven

@@ -56,6 +56,11 @@ class Accum(C.Structure):
     _fields_ = [(n, dbl_p) for n in ACCUM_FIELDS] + [(n, C.c_int32) for n in ("n_ts", "n_uv", "n_w", "n_ch", "n_ssh")]
 
 
+class CnnStats(C.Structure):
+    _fields_ = [("in_mean", C.c_float * 5), ("in_std", C.c_float * 5), ("out_std", C.c_float * 4),
+                ("alpha_ref", C.c_double * 64)]
+
+
 class TropIO(C.Structure):
     _fields_ = [("glo_ni", C.c_int32), ("glo_nj", C.c_int32), ("dtbt", C.c_int32), ("dtbc", C.c_int32),
                 ("flags", C.c_int32), ("lev_t", C.c_void_p), ("lev_u", C.c_void_p),
@@ -102,6 +107,10 @@ SIGNATURES = {
     "pcom_gpu_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
     "pcom_gpu_trop_noalloc": (C.c_int, [C.POINTER(TropIO), C.c_void_p]),
     "pcom_gpu_global_sums": (C.c_int, [C.c_void_p, dbl_p]),
+    "pcom_gpu_coarsen": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "pcom_gpu_cnn_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pcom_gpu_cnn_target": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
+    "pcom_gpu_cnn_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "pcom_gpu_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
     "pcom_gpu_batch_destroy": (C.c_int, [C.c_void_p]),
     "pcom_gpu_batch_step": (C.c_int, [C.c_void_p, C.c_int64]),

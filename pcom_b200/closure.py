@@ -1,0 +1,323 @@
+"""The learned subgrid closure: data from a fine run coarse-grained onto a
+nested coarse grid, training of the tensor-core network (include/pcom_cnn.h)
+and coarse runs with and without it.
+
+Target.  For a sample time t the coarse model is started from the
+coarse-grained fine state CG(fine(t)) and stepped once (dt = the coarse
+baroclinic step); the target is the per-level tendency residual
+    (CG(fine(t + dt)) - coarse_step(CG(fine(t)))) / dt
+for u, v, T and S, the part of the fine model's evolution the coarse model
+misses.  Inputs: u, v, T, S and the specific-volume anomaly per level, as
+5 channels of one image per level.  Closure run: after every coarse step the
+network's output (scaled back) is added as a tendency over the step.
+
+Usage (the experiment reported for the 1-degree grid):
+    python -m pcom_b200.closure --fine global025 --spinup-days 2 \
+        --train-days 8 --eval-days 2 --out closure_result.json
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import _lib as L
+from .model import Model
+from .synth import make_case
+
+STEP = 3600  # coarse baroclinic step (s)
+
+
+def _check_cnn(rc, what):
+    if rc != 0:
+        buf = C.create_string_buffer(512)
+        L.load().pcom_cnn_last_error(buf, 512)
+        raise L.PcomError(f"{what}: {buf.value.decode(errors='replace')}")
+
+
+def coarse_case(fine: dict, factor: int = 4) -> dict:
+    """The nested coarse grid of a fine case: lon block means, every
+    factor-th north edge in lat, each coarse column as deep as the
+    shallowest fine column of its block, block-mean initial state and
+    forcing; dtbt 60 s, dtbc 3600 s."""
+    f = factor
+    ni, nj, nk = fine["glo_ni"] // f, fine["glo_nj"] // f, fine["nk"]
+    blk = lambda a: a.reshape(a.shape[:-2] + (nj, f, ni, f)).mean(axis=(-3, -1))
+    itn = fine["itn"].reshape(nj, f, ni, f).min(axis=(1, 3)).astype(np.int32)
+    c = dict(fine)
+    c.update(name=fine["name"] + f"_c{f}", glo_ni=ni, glo_nj=nj, dtbt=60, dtbc=STEP,
+             lon=fine["lon"].reshape(ni, f).mean(axis=1), lat=fine["lat"][f - 1::f].copy(), itn=itn,
+             pt=blk(fine["pt"]), sa=blk(fine["sa"]))
+    for k in ("taux", "tauy", "bct", "bcs", "pa", "fw"):
+        c[k] = blk(fine[k])
+    return c
+
+
+class Network:
+    """The tensor-core network on device buffers for `nimg` images of H x W."""
+
+    def __init__(self, H: int, W: int, nimg: int, periodic_x: bool = True, seed: int = 0):
+        self.lib = L.load()
+        self.H, self.W, self.nimg = H, W, nimg
+        self.h = C.c_void_p()
+        _check_cnn(self.lib.pcom_cnn_create(H, W, nimg, 1 if periodic_x else 0, C.byref(self.h)), "pcom_cnn_create")
+        self.nparam = int(self.lib.pcom_cnn_param_count())
+        rng = np.random.default_rng(seed)
+        par = np.zeros(self.nparam, np.float32)
+        o = 0
+        for li, (k, n) in enumerate(((16, 64), (64, 64), (64, 64), (64, 64), (64, 16))):
+            std = np.sqrt(2.0 / (9 * (5 if li == 0 else k)))
+            if li == 4:
+                std *= 0.1  # start close to the plain model (zero tendency)
+            par[o:o + 9 * n * k] = rng.standard_normal(9 * n * k) * std
+            o += 9 * n * k + n
+        self.set_params(par)
+
+    def set_params(self, par):
+        par = np.ascontiguousarray(par, np.float32)
+        _check_cnn(self.lib.pcom_cnn_set_params(self.h, par.ctypes.data, par.size), "set_params")
+
+    def params(self):
+        out = np.zeros(self.nparam, np.float32)
+        _check_cnn(self.lib.pcom_cnn_get_params(self.h, out.ctypes.data, out.size), "get_params")
+        return out
+
+    def set_stream(self, ptr: int):
+        _check_cnn(self.lib.pcom_cnn_set_stream(self.h, C.c_void_p(ptr)), "set_stream")
+
+    def train_step(self, x, target, mask, lr) -> float:
+        loss = C.c_double()
+        _check_cnn(self.lib.pcom_cnn_train_step(self.h, x.data_ptr(), target.data_ptr(), mask.data_ptr(), self.nimg,
+                                                C.c_float(lr), C.byref(loss)), "train_step")
+        return loss.value
+
+    def loss(self, x, target, mask) -> float:
+        loss = C.c_double()
+        _check_cnn(self.lib.pcom_cnn_gradient(self.h, x.data_ptr(), target.data_ptr(), mask.data_ptr(), self.nimg,
+                                              None, C.byref(loss)), "gradient")
+        return loss.value
+
+    def forward(self, x, y):
+        _check_cnn(self.lib.pcom_cnn_forward(self.h, x.data_ptr(), y.data_ptr(), self.nimg), "forward")
+
+    def close(self):
+        if self.h and self.h.value:
+            self.lib.pcom_cnn_destroy(self.h)
+            self.h = C.c_void_p()
+
+
+def _stats_struct(st: dict) -> L.CnnStats:
+    s = L.CnnStats()
+    for q in range(5):
+        s.in_mean[q] = st["in_mean"][q]
+        s.in_std[q] = st["in_std"][q]
+    for q in range(4):
+        s.out_std[q] = st["out_std"][q]
+    for k, v in enumerate(st["alpha_ref"]):
+        s.alpha_ref[k] = v
+    return s
+
+
+class Experiment:
+    """Fine model, two coarse models on the nested grid (prediction and
+    coarse-grained truth) and the data they produce."""
+
+    def __init__(self, fine_case: dict, factor: int = 4):
+        import torch
+
+        self.torch = torch
+        self.lib = L.load()
+        self.factor = factor
+        self.fine = Model(fine_case)
+        self.fc = fine_case
+        self.cc = coarse_case(fine_case, factor)
+        self.pred = Model(self.cc)
+        self.truth = Model(self.cc)
+        for m in (self.pred, self.truth):
+            m.set_forcing(m.int_bnd())
+        self.nk, self.H, self.W = self.cc["nk"], self.cc["glo_nj"], self.cc["glo_ni"]
+        self.npix = self.nk * self.H * self.W
+        self.fine_steps = STEP // fine_case["dtbc"]
+        self.stats = None
+        self.citer = 100  # coarse iteration numbers past the AB3 start-up
+
+    def coarsen(self, into: Model):
+        L.check(self.lib.pcom_gpu_coarsen(self.fine.handle, into.handle, self.factor), "coarsen")
+
+    def _features(self, m: Model, x):
+        L.check(self.lib.pcom_gpu_cnn_features(m.handle, C.c_void_p(x.data_ptr()), C.byref(self.st)), "features")
+        m.sync()
+
+    def compute_stats(self):
+        """Input normalisation from the current coarse-grained fine state and
+        output scales from one target sample."""
+        torch = self.torch
+        self.coarsen(self.pred)
+        st = self.pred.static()
+        k = np.arange(1, self.nk + 1)[:, None, None]
+        wt, wu = st["lev_t"][None] >= k, st["lev_u"][None] >= k
+        alpha = self.pred.field("alpha")
+        aref = [float(alpha[q][wt[q]].mean()) if wt[q].any() else 0.0 for q in range(self.nk)]
+        an = alpha - np.array(aref)[:, None, None]
+        fields = [(self.pred.field("uc"), wu), (self.pred.field("vc"), wu), (self.pred.field("tc"), wt),
+                  (self.pred.field("sc"), wt), (an, wt)]
+        mean = [float(f[w].mean()) for f, w in fields]
+        std = [float(f[w].std()) or 1.0 for f, w in fields]
+        self.stats = dict(in_mean=mean, in_std=std, out_std=[1.0] * 4, alpha_ref=aref)
+        self.st = _stats_struct(self.stats)
+        # output scales from one unscaled target
+        t = torch.zeros((self.npix, 4), dtype=torch.float32, device="cuda")
+        mk = torch.zeros((self.npix, 4), dtype=torch.float32, device="cuda")
+        self._one_target(t, mk)
+        tn, mn = t.cpu().numpy(), mk.cpu().numpy()
+        self.stats["out_std"] = [float(np.sqrt((tn[:, q] ** 2 * mn[:, q]).sum() / max(mn[:, q].sum(), 1))) or 1.0
+                                 for q in range(4)]
+        self.st = _stats_struct(self.stats)
+
+    def _one_target(self, target, mask, x=None):
+        """From the fine model's current time t: features of CG(fine(t)) into
+        x, the coarse step from it, the fine model advanced to t + dt, and the
+        residual into target.  The fine model ends at t + dt."""
+        self.coarsen(self.pred)
+        self.pred.den_prho()
+        if x is not None:
+            self._features(self.pred, x)
+        self.citer += 1
+        self.pred.step_handle(self.citer)
+        self.fine.run(self.fine_steps)
+        self.coarsen(self.truth)
+        L.check(self.lib.pcom_gpu_cnn_target(self.pred.handle, self.truth.handle, C.c_void_p(target.data_ptr()),
+                                             C.c_void_p(mask.data_ptr()), C.byref(self.st), float(STEP)), "target")
+        self.pred.sync()
+
+    def generate(self, nsamples: int, every: int = 1):
+        """nsamples (x, target) pairs, one every `every` coarse steps."""
+        torch = self.torch
+        xs = torch.zeros((nsamples, self.npix, 16), dtype=torch.bfloat16, device="cuda")
+        ts = torch.zeros((nsamples, self.npix, 4), dtype=torch.float32, device="cuda")
+        mask = torch.zeros((self.npix, 4), dtype=torch.float32, device="cuda")
+        for s in range(nsamples):
+            for _ in range(every - 1):
+                self.fine.run(self.fine_steps)
+            self._one_target(ts[s], mask, xs[s])
+        return xs, ts, mask
+
+
+def train(net: Network, xs, ts, mask, epochs: int, lr: float, val_frac: float = 0.2, log=print):
+    """Adam over the samples (one sample = all levels = one step); returns
+    training and validation curves and the zero-prediction baseline."""
+    n = xs.shape[0]
+    nval = max(1, int(round(n * val_frac)))
+    ntr = n - nval
+    order = np.arange(ntr)
+    rng = np.random.default_rng(0)
+    base = [float(((ts[s] ** 2) * mask).sum() / mask.sum()) for s in range(ntr, n)]
+    hist = []
+    for ep in range(epochs):
+        rng.shuffle(order)
+        tr = [net.train_step(xs[s], ts[s], mask, lr) for s in order]
+        val = [net.loss(xs[s], ts[s], mask) for s in range(ntr, n)]
+        hist.append((float(np.mean(tr)), float(np.mean(val))))
+        log(f"epoch {ep + 1}: train {hist[-1][0]:.4f}  val {hist[-1][1]:.4f}  (zero-output {np.mean(base):.4f})")
+    return dict(history=hist, val_zero_baseline=float(np.mean(base)), ntrain=ntr, nval=nval)
+
+
+def coarse_rms(exp: Experiment, m: Model) -> dict:
+    """RMS difference of u, v, T, S between a coarse model and CG(fine)."""
+    exp.coarsen(exp.truth)
+    st = m.static()
+    k = np.arange(1, exp.nk + 1)[:, None, None]
+    wt, wu = st["lev_t"][None] >= k, st["lev_u"][None] >= k
+    out = {}
+    for f, w in (("uc", wu), ("vc", wu), ("tc", wt), ("sc", wt)):
+        d = (m.field(f) - exp.truth.field(f))[w]
+        out[f] = float(np.sqrt(np.mean(d * d)))
+    return out
+
+
+def evaluate(exp: Experiment, net: Network, steps: int, apply_every: int = 1):
+    """Coarse runs from CG(fine(t0)) with and without the closure for
+    `steps` coarse steps beside the fine run; RMS error against
+    CG(fine(t)) at the end, and timings."""
+    torch = exp.torch
+    plain, clos = Model(exp.cc), Model(exp.cc)
+    for m in (plain, clos):
+        m.set_forcing(m.int_bnd())
+        exp.coarsen(m)
+    x = torch.zeros((exp.npix, 16), dtype=torch.bfloat16, device="cuda")
+    y = torch.zeros((exp.npix, 4), dtype=torch.float32, device="cuda")
+    it = 100
+    t_plain = t_clos = 0.0
+    for s in range(steps):
+        it += 1
+        day = (s % 24 == 0)
+        t0 = time.perf_counter()
+        if day:
+            plain.den_prho()
+        plain.step_handle(it)
+        t_plain += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        if day:
+            clos.den_prho()
+        clos.step_handle(it)
+        if (s + 1) % apply_every == 0:
+            exp._features(clos, x)
+            net.forward(x, y)
+            L.check(exp.lib.pcom_gpu_cnn_apply(clos.handle, C.c_void_p(y.data_ptr()), C.byref(exp.st),
+                                               float(STEP * apply_every)), "apply")
+            clos.sync()
+        t_clos += time.perf_counter() - t0
+        exp.fine.run(exp.fine_steps)
+    clos.check_finite()
+    res = dict(steps=steps, rms_plain=coarse_rms(exp, plain), rms_closure=coarse_rms(exp, clos),
+               s_per_step_plain=t_plain / steps, s_per_step_closure=t_clos / steps)
+    plain.close()
+    clos.close()
+    return res
+
+
+def main():
+    import torch
+
+    p = argparse.ArgumentParser()
+    p.add_argument("--fine", default="global025")
+    p.add_argument("--factor", type=int, default=4)
+    p.add_argument("--spinup-days", type=float, default=2)
+    p.add_argument("--train-days", type=float, default=8)
+    p.add_argument("--every", type=int, default=2)
+    p.add_argument("--eval-days", type=float, default=2)
+    p.add_argument("--epochs", type=int, default=8)
+    p.add_argument("--lr", type=float, default=1e-3)
+    p.add_argument("--out", default=None)
+    a = p.parse_args()
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    exp = Experiment(make_case(a.fine), a.factor)
+    fine_spd = 86400 // exp.fc["dtbc"]
+    tf = time.perf_counter()
+    exp.fine.run(int(a.spinup_days * fine_spd))
+    exp.fine.sync()
+    fine_s_per_step = (time.perf_counter() - tf) / max(1, int(a.spinup_days * fine_spd))
+    exp.compute_stats()
+    nsamp = int(a.train_days * 24 / a.every)
+    xs, ts, mask = exp.generate(nsamp, a.every)
+    net = Network(exp.H, exp.W, exp.nk)
+    tt = time.perf_counter()
+    tr = train(net, xs, ts, mask, a.epochs, a.lr)
+    t_train = time.perf_counter() - tt
+    ev = evaluate(exp, net, int(a.eval_days * 24))
+    res = dict(fine=a.fine, coarse_grid=[exp.W, exp.H, exp.nk], samples=nsamp, epochs=a.epochs,
+               train=tr, train_seconds=t_train, eval=ev, stats=exp.stats, fine_s_per_step=fine_s_per_step,
+               fine_steps_per_coarse_step=exp.fine_steps, wall_seconds=time.time() - t0)
+    line = json.dumps(res)
+    print(line)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

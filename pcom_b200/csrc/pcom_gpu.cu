@@ -8,6 +8,7 @@
 // (mod_int.f90:115-118) rotates three buffers per component, and int_ts
 // writes the new T/S into a free buffer that then becomes both tc and tp
 // (mod_int.f90:496-497).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -181,6 +182,106 @@ __global__ void k_sums_final(const double *part, int nb, double *out) {
   for (int b = 0; b < nb; ++b)
     for (int c = 0; c < 3; ++c) a[c] += part[3 * b + c];
   for (int c = 0; c < 3; ++c) out[c] = a[c];
+}
+
+// ---- closure coupling (FP64 handles)
+struct Grid2 {
+  int ni, glo_ni, glo_nj, nk;
+  long long n2;
+};
+__device__ __forceinline__ void put_twin(double *f, const Grid2 &g, int i, long long q, double v) {
+  f[q] = v;
+  if (i == 2) f[q + (g.ni - 2)] = v;
+  else if (i == g.ni - 1) f[q - (g.ni - 2)] = v;
+}
+// block mean over wet fine cells (all cells when none is wet) of nlev planes
+__global__ void k_coarsen(const double *f, double *c, const int *levf, Grid2 F, Grid2 Cg, int nlev, int factor,
+                          int plane_lev) {
+  const long long n = (long long)Cg.glo_ni * Cg.glo_nj * nlev;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(p % Cg.glo_ni), J = (int)((p / Cg.glo_ni) % Cg.glo_nj), k = (int)(p / ((long long)Cg.glo_ni * Cg.glo_nj)) + 1;
+    const int kl = plane_lev ? k : 1;
+    double sw = 0.0, sa = 0.0;
+    int nw = 0;
+    for (int b = 0; b < factor; ++b)
+      for (int a = 0; a < factor; ++a) {
+        const long long q2 = (long long)(1 + factor * I + a) + (long long)F.ni * (1 + factor * J + b);
+        const double v = f[q2 + F.n2 * (k - 1)];
+        sa += v;
+        if (levf[q2] >= kl) { sw += v; ++nw; }
+      }
+    const double m = nw ? sw / nw : sa / (factor * factor);
+    const int i = I + 2;
+    const long long q = (long long)(i - 1) + (long long)Cg.ni * (J + 1) + Cg.n2 * (k - 1);
+    put_twin(c, Cg, i, q, m);
+  }
+}
+struct CnnStatsDev {
+  float in_mean[5], in_std[5], out_std[4];
+  double alpha_ref[64];
+};
+__global__ void k_cnn_features(const __grid_constant__ Dev P, __nv_bfloat16 *x, CnnStatsDev st) {
+  const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(p % P.glo_ni), J = (int)((p / P.glo_ni) % P.glo_nj), k = (int)(p / ((long long)P.glo_ni * P.glo_nj)) + 1;
+    const long long q2 = (long long)(I + 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
+    const bool wu = P.lev_u[q2] >= k, wt = P.lev_t[q2] >= k;
+    float v[5];
+    v[0] = wu ? (float)((P.uc[q] - st.in_mean[0]) / st.in_std[0]) : 0.f;
+    v[1] = wu ? (float)((P.vc[q] - st.in_mean[1]) / st.in_std[1]) : 0.f;
+    v[2] = wt ? (float)((P.tc[q] - st.in_mean[2]) / st.in_std[2]) : 0.f;
+    v[3] = wt ? (float)((P.sc[q] - st.in_mean[3]) / st.in_std[3]) : 0.f;
+    v[4] = wt ? (float)((P.alpha[q] - st.alpha_ref[k - 1] - st.in_mean[4]) / st.in_std[4]) : 0.f;
+    __nv_bfloat16 *o = x + p * 16;
+    #pragma unroll
+    for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16(c < 5 ? v[c] : 0.f);
+  }
+}
+__global__ void k_cnn_target(const __grid_constant__ Dev Pp, const __grid_constant__ Dev Pt, float *target, float *mask,
+                             CnnStatsDev st, double rdt) {
+  const long long n = (long long)Pp.glo_ni * Pp.glo_nj * Pp.nk;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(p % Pp.glo_ni), J = (int)((p / Pp.glo_ni) % Pp.glo_nj), k = (int)(p / ((long long)Pp.glo_ni * Pp.glo_nj)) + 1;
+    const long long q2 = (long long)(I + 1) + (long long)Pp.ni * (J + 1), q = q2 + Pp.n2 * (k - 1);
+    const float mu = Pp.lev_u[q2] >= k ? 1.f : 0.f, mt = Pp.lev_t[q2] >= k ? 1.f : 0.f;
+    if (target) {
+      target[p * 4 + 0] = mu * (float)((Pt.uc[q] - Pp.uc[q]) * rdt / st.out_std[0]);
+      target[p * 4 + 1] = mu * (float)((Pt.vc[q] - Pp.vc[q]) * rdt / st.out_std[1]);
+      target[p * 4 + 2] = mt * (float)((Pt.tc[q] - Pp.tc[q]) * rdt / st.out_std[2]);
+      target[p * 4 + 3] = mt * (float)((Pt.sc[q] - Pp.sc[q]) * rdt / st.out_std[3]);
+    }
+    if (mask) {
+      mask[p * 4 + 0] = mu;
+      mask[p * 4 + 1] = mu;
+      mask[p * 4 + 2] = mt;
+      mask[p * 4 + 3] = mt;
+    }
+  }
+}
+__global__ void k_cnn_apply(const __grid_constant__ Dev P, const float *y, CnnStatsDev st, double dt, int tp_distinct) {
+  const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
+  const Grid2 G{P.ni, P.glo_ni, P.glo_nj, P.nk, P.n2};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(p % P.glo_ni), J = (int)((p / P.glo_ni) % P.glo_nj), k = (int)(p / ((long long)P.glo_ni * P.glo_nj)) + 1;
+    const int i = I + 2;
+    const long long q2 = (long long)(i - 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
+    if (P.lev_u[q2] >= k) {
+      const double du = dt * st.out_std[0] * y[p * 4 + 0], dv = dt * st.out_std[1] * y[p * 4 + 1];
+      put_twin(P.uc, G, i, q, P.uc[q] + du);
+      put_twin(P.vc, G, i, q, P.vc[q] + dv);
+      put_twin(P.up, G, i, q, P.up[q] + du);
+      put_twin(P.vp, G, i, q, P.vp[q] + dv);
+    }
+    if (P.lev_t[q2] >= k) {
+      const double dT = dt * st.out_std[2] * y[p * 4 + 2], dS = dt * st.out_std[3] * y[p * 4 + 3];
+      put_twin(P.tc, G, i, q, P.tc[q] + dT);
+      put_twin(P.sc, G, i, q, P.sc[q] + dS);
+      if (tp_distinct) {
+        put_twin(P.tp, G, i, q, P.tp[q] + dT);
+        put_twin(P.sp, G, i, q, P.sp[q] + dS);
+      }
+    }
+  }
 }
 
 struct ProfEntry {
@@ -1138,6 +1239,78 @@ int pcom_gpu_global_sums(pcom_handle *h, double *out3) {
   h->launches += 2;
   CK(cudaMemcpyAsync(out3, h->d_sums + 3 * nb, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   return sync_check(h);
+}
+
+namespace {
+CnnStatsDev stats_dev(const pcom_cnn_stats *s) {
+  CnnStatsDev d{};
+  memcpy(d.in_mean, s->in_mean, sizeof d.in_mean);
+  memcpy(d.in_std, s->in_std, sizeof d.in_std);
+  memcpy(d.out_std, s->out_std, sizeof d.out_std);
+  memcpy(d.alpha_ref, s->alpha_ref, sizeof d.alpha_ref);
+  return d;
+}
+Grid2 grid2(const pcom_handle *h) { return Grid2{h->ni, h->dims.glo_ni, h->dims.glo_nj, h->nk, h->n2}; }
+}  // namespace
+
+int pcom_gpu_coarsen(pcom_handle *f, pcom_handle *c, int32_t factor) {
+  if (!f || !c || factor < 1) return fail(PCOM_ERR_ARG, "null handle or factor < 1");
+  if (f->mixed || c->mixed) return fail(PCOM_ERR_ARG, "coarsening runs on FP64 handles");
+  if (!f->static_ok || !c->static_ok) return fail(PCOM_ERR_STATE, "static data missing");
+  if (f->dims.glo_ni != factor * c->dims.glo_ni || f->dims.glo_nj != factor * c->dims.glo_nj || f->nk != c->nk)
+    return fail(PCOM_ERR_ARG, "grids do not nest with factor %d", factor);
+  CK(cudaStreamSynchronize(f->stream));
+  const Grid2 F = grid2(f), Cg = grid2(c);
+  Dev &A = f->D, &B = c->D;
+  const int nk = c->nk;
+  auto run = [&](const double *src, double *dst, const int *lev, int nlev, int plane) {
+    k_coarsen<<<592, 256, 0, c->stream>>>(src, dst, lev, F, Cg, nlev, factor, plane);
+  };
+  run(A.tc, B.tc, A.lev_t, nk, 1);
+  run(A.sc, B.sc, A.lev_t, nk, 1);
+  if (B.tp != B.tc) { run(A.tp, B.tp, A.lev_t, nk, 1); run(A.sp, B.sp, A.lev_t, nk, 1); }
+  const double *fu[] = {A.uc, A.vc, A.up, A.vp, A.auc, A.aup, A.aupp, A.avc, A.avp, A.avpp, A.am};
+  double *cu[] = {B.uc, B.vc, B.up, B.vp, B.auc, B.aup, B.aupp, B.avc, B.avp, B.avpp, B.am};
+  for (int q = 0; q < 11; ++q) run(fu[q], cu[q], A.lev_u, nk, 1);
+  const double *ft[] = {A.chc, A.chp, A.mch, A.mch2};
+  double *ct[] = {B.chc, B.chp, B.mch, B.mch2};
+  for (int q = 0; q < 4; ++q) run(ft[q], ct[q], A.lev_t, 1, 0);
+  const double *fb[] = {A.ubc, A.vbc, A.ubp, A.vbp};
+  double *cb[] = {B.ubc, B.vbc, B.ubp, B.vbp};
+  for (int q = 0; q < 4; ++q) run(fb[q], cb[q], A.lev_u, 1, 0);
+  CK(cudaGetLastError());
+  c->launches += 21;
+  return sync_check(c);
+}
+
+int pcom_gpu_cnn_features(pcom_handle *h, void *x, const pcom_cnn_stats *st) {
+  if (!h || !x || !st) return fail(PCOM_ERR_ARG, "null argument");
+  if (h->mixed) return fail(PCOM_ERR_ARG, "closure features are built from FP64 handles");
+  k_cnn_features<<<592, 256, 0, h->stream>>>(h->D, (__nv_bfloat16 *)x, stats_dev(st));
+  CK(cudaGetLastError());
+  h->launches++;
+  return PCOM_OK;
+}
+
+int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, float *mask, const pcom_cnn_stats *st,
+                        double dt) {
+  if (!pred || !truth || !st || dt <= 0) return fail(PCOM_ERR_ARG, "bad argument");
+  if (pred->mixed || truth->mixed) return fail(PCOM_ERR_ARG, "closure targets are built from FP64 handles");
+  if (pred->n3 != truth->n3) return fail(PCOM_ERR_ARG, "handles differ in size");
+  CK(cudaStreamSynchronize(truth->stream));
+  k_cnn_target<<<592, 256, 0, pred->stream>>>(pred->D, truth->D, target, mask, stats_dev(st), 1.0 / dt);
+  CK(cudaGetLastError());
+  pred->launches++;
+  return PCOM_OK;
+}
+
+int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *st, double dt) {
+  if (!h || !y || !st) return fail(PCOM_ERR_ARG, "null argument");
+  if (h->mixed) return fail(PCOM_ERR_ARG, "the closure is applied on FP64 handles");
+  k_cnn_apply<<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
+  CK(cudaGetLastError());
+  h->launches++;
+  return PCOM_OK;
 }
 
 int pcom_gpu_set_stream(pcom_handle *h, void *stream) {
