@@ -41,6 +41,24 @@ def sypd(seconds_per_step: float) -> float:
     return (86400.0 / seconds_per_step) / YEAR_STEPS
 
 
+def max_over_ranks(t_ms: float, world: int, device: str) -> float:
+    """The slowest rank's time (every rank takes part in the collective)."""
+    if world <= 1:
+        return t_ms
+    import torch
+    import torch.distributed as dist
+
+    tt = torch.tensor([t_ms], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_sypd(ms_per_step: float, world: int) -> float:
+    """Whole-job SYPD of `world` replicas (one member per rank), each step
+    timed as the max over ranks: every rank advanced its member by one step."""
+    return world * sypd(ms_per_step / 1000.0)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -206,13 +224,9 @@ def run_ours(args):
     prof = m.profile_read()
     m.profile(False)
     L.check(lib.pcom_gpu_check_finite(h), "watchdog")
-    t_max = t_ms
-    if world > 1:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max = max_over_ranks(t_ms, world, "cuda")
     ms_per_step = t_max / steps
-    value = world * sypd(ms_per_step / 1000.0)
+    value = replica_sypd(ms_per_step, world)
 
     # ------------------------------------------------ e2e: host buffers
     # per step through the reference-facing API: the day's forcing from pinned
@@ -243,12 +257,8 @@ def run_ours(args):
         L.check(lib.pcom_gpu_get_state(h, C.byref(st_out)), "get_state")
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = world * sypd(e2e_ms / steps / 1000.0)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
+    e2e = replica_sypd(e2e_ms / steps, world)
 
     # ------------------------------------------------ roofline of the dominant kernel
     peaks = {}

@@ -155,6 +155,12 @@ int64_t pcom_gpu_field_size(pcom_handle *h, const char *name);
 /* Run the NaN/Inf watchdog over the prognostic fields; PCOM_ERR_NUMERIC if
  * any wet point is not finite. */
 int pcom_gpu_check_finite(pcom_handle *h);
+/* Barotropic kernel choice: 0 automatic (resident when the domain's tiles
+ * fit one per CTA, else multi-tile), 1 resident (one region point per
+ * thread, coefficients in registers), 2 multi-tile (several tiles per CTA),
+ * 3 generic (non-separable metrics).  All give the same results; the choice
+ * is for tuning and tests.  No counterpart in the reference. */
+int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which);
 /* Global sums over the wet T cells of the interior: out3[0] = volume (m^3),
  * out3[1] = sum of T dV (K m^3), out3[2] = sum of S dV (psu m^3), with
  * dV = a^2 rh1 dx1x dx1y dz(k); FP64, in a fixed reduction order.  No
@@ -179,6 +185,8 @@ int64_t pcom_gpu_launch_count(pcom_handle *h);
 typedef struct {
   float in_mean[5], in_std[5];  /* u, v, T, S, alpha - alpha_ref(k) */
   float out_std[4];             /* du, dv, dT, dS tendency scales */
+  float out_gain[4];            /* applied fraction per output (pcom_gpu_cnn_apply) */
+  float out_clip;               /* |y| limit in units of out_std (0: none) */
   double alpha_ref[64];         /* [k - 1], k = 1..nk */
 } pcom_cnn_stats;
 /* Set the coarse handle's state to the block means (factor x factor) of the
@@ -198,8 +206,9 @@ int pcom_gpu_cnn_features(pcom_handle *h, void *x_bf16, const pcom_cnn_stats *st
 int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, float *mask, const pcom_cnn_stats *stats,
                         double dt);
 /* Apply the network's output y (FP32 [nk][glo_nj][glo_ni][4], device) as a
- * tendency over dt seconds: uc, up += dt out_std[0] y0 (wet U points), vc,
- * vp likewise, tc, tp, sc, sp on wet T cells. */
+ * tendency over dt seconds: uc, up += dt out_gain[0] out_std[0] y0 (wet U
+ * points, y clipped to +-out_clip when out_clip > 0), vc, vp likewise, tc,
+ * tp, sc, sp on wet T cells. */
 int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *stats, double dt);
 
 /* --- batches -------------------------------------------------------------- */

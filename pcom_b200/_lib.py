@@ -58,7 +58,7 @@ class Accum(C.Structure):
 
 class CnnStats(C.Structure):
     _fields_ = [("in_mean", C.c_float * 5), ("in_std", C.c_float * 5), ("out_std", C.c_float * 4),
-                ("alpha_ref", C.c_double * 64)]
+                ("out_gain", C.c_float * 4), ("out_clip", C.c_float), ("alpha_ref", C.c_double * 64)]
 
 
 class TropIO(C.Structure):
@@ -107,6 +107,7 @@ SIGNATURES = {
     "pcom_gpu_last_error": (C.c_int, [C.c_char_p, C.c_int32]),
     "pcom_gpu_trop_noalloc": (C.c_int, [C.POINTER(TropIO), C.c_void_p]),
     "pcom_gpu_global_sums": (C.c_int, [C.c_void_p, dbl_p]),
+    "pcom_gpu_set_trop_kernel": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_coarsen": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "pcom_gpu_cnn_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pcom_gpu_cnn_target": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),

@@ -116,6 +116,8 @@ def _stats_struct(st: dict) -> L.CnnStats:
         s.in_std[q] = st["in_std"][q]
     for q in range(4):
         s.out_std[q] = st["out_std"][q]
+        s.out_gain[q] = st.get("out_gain", [1.0] * 4)[q]
+    s.out_clip = st.get("out_clip", 0.0)
     for k, v in enumerate(st["alpha_ref"]):
         s.alpha_ref[k] = v
     return s
@@ -125,7 +127,7 @@ class Experiment:
     """Fine model, two coarse models on the nested grid (prediction and
     coarse-grained truth) and the data they produce."""
 
-    def __init__(self, fine_case: dict, factor: int = 4):
+    def __init__(self, fine_case: dict, factor: int = 4, target_steps: int = 1):
         import torch
 
         self.torch = torch
@@ -143,6 +145,7 @@ class Experiment:
         self.fine_steps = STEP // fine_case["dtbc"]
         self.stats = None
         self.citer = 100  # coarse iteration numbers past the AB3 start-up
+        self.kt = target_steps  # coarse steps the residual is accumulated over
 
     def coarsen(self, into: Model):
         L.check(self.lib.pcom_gpu_coarsen(self.fine.handle, into.handle, self.factor), "coarsen")
@@ -179,28 +182,31 @@ class Experiment:
 
     def _one_target(self, target, mask, x=None):
         """From the fine model's current time t: features of CG(fine(t)) into
-        x, the coarse step from it, the fine model advanced to t + dt, and the
-        residual into target.  The fine model ends at t + dt."""
+        x, kt coarse steps from it, the fine model advanced to t + kt dt, and
+        the mean residual tendency into target.  The fine model ends at
+        t + kt dt."""
         self.coarsen(self.pred)
         self.pred.den_prho()
         if x is not None:
             self._features(self.pred, x)
-        self.citer += 1
-        self.pred.step_handle(self.citer)
-        self.fine.run(self.fine_steps)
+        for _ in range(self.kt):
+            self.citer += 1
+            self.pred.step_handle(self.citer)
+        self.fine.run(self.fine_steps * self.kt)
         self.coarsen(self.truth)
         L.check(self.lib.pcom_gpu_cnn_target(self.pred.handle, self.truth.handle, C.c_void_p(target.data_ptr()),
-                                             C.c_void_p(mask.data_ptr()), C.byref(self.st), float(STEP)), "target")
+                                             C.c_void_p(mask.data_ptr()), C.byref(self.st), float(STEP * self.kt)),
+                "target")
         self.pred.sync()
 
     def generate(self, nsamples: int, every: int = 1):
-        """nsamples (x, target) pairs, one every `every` coarse steps."""
+        """nsamples (x, target) pairs, one every max(every, kt) coarse steps."""
         torch = self.torch
         xs = torch.zeros((nsamples, self.npix, 16), dtype=torch.bfloat16, device="cuda")
         ts = torch.zeros((nsamples, self.npix, 4), dtype=torch.float32, device="cuda")
         mask = torch.zeros((self.npix, 4), dtype=torch.float32, device="cuda")
         for s in range(nsamples):
-            for _ in range(every - 1):
+            for _ in range(every - self.kt):
                 self.fine.run(self.fine_steps)
             self._one_target(ts[s], mask, xs[s])
         return xs, ts, mask
@@ -238,19 +244,36 @@ def coarse_rms(exp: Experiment, m: Model) -> dict:
     return out
 
 
-def evaluate(exp: Experiment, net: Network, steps: int, apply_every: int = 1):
-    """Coarse runs from CG(fine(t0)) with and without the closure for
-    `steps` coarse steps beside the fine run; RMS error against
-    CG(fine(t)) at the end, and timings."""
+VARIANTS = {  # applied fraction of each output (du, dv, dT, dS) and the |y| clip
+    "all": ([1.0, 1.0, 1.0, 1.0], 3.0),
+    "tracers": ([0.0, 0.0, 1.0, 1.0], 3.0),
+    "tracers+0.25uv": ([0.25, 0.25, 1.0, 1.0], 3.0),
+}
+
+
+def evaluate(exp: Experiment, net: Network, steps: int, variants=VARIANTS):
+    """Coarse runs from CG(fine(t0)) beside the fine run for `steps` coarse
+    steps: the plain coarse model and, per variant, the model with the
+    closure applied after every step.  A closure run whose state stops being
+    finite falls back to the plain model (its state is replaced by the plain
+    run's and the closure is switched off).  RMS error against CG(fine(t))
+    at the end, and the time per step with and without the network."""
     torch = exp.torch
-    plain, clos = Model(exp.cc), Model(exp.cc)
-    for m in (plain, clos):
+    plain = Model(exp.cc)
+    runs = {v: Model(exp.cc) for v in variants}
+    stats = {}
+    for v, (gain, clip) in variants.items():
+        st = dict(exp.stats, out_gain=gain, out_clip=clip)
+        stats[v] = _stats_struct(st)
+    for m in [plain] + list(runs.values()):
         m.set_forcing(m.int_bnd())
         exp.coarsen(m)
     x = torch.zeros((exp.npix, 16), dtype=torch.bfloat16, device="cuda")
     y = torch.zeros((exp.npix, 4), dtype=torch.float32, device="cuda")
+    active = {v: True for v in variants}
+    fallback = {v: None for v in variants}
     it = 100
-    t_plain = t_clos = 0.0
+    t_plain = t_net = 0.0
     for s in range(steps):
         it += 1
         day = (s % 24 == 0)
@@ -259,23 +282,36 @@ def evaluate(exp: Experiment, net: Network, steps: int, apply_every: int = 1):
             plain.den_prho()
         plain.step_handle(it)
         t_plain += time.perf_counter() - t0
-        t0 = time.perf_counter()
-        if day:
-            clos.den_prho()
-        clos.step_handle(it)
-        if (s + 1) % apply_every == 0:
-            exp._features(clos, x)
-            net.forward(x, y)
-            L.check(exp.lib.pcom_gpu_cnn_apply(clos.handle, C.c_void_p(y.data_ptr()), C.byref(exp.st),
-                                               float(STEP * apply_every)), "apply")
-            clos.sync()
-        t_clos += time.perf_counter() - t0
+        for v, m in runs.items():
+            if day:
+                m.den_prho()
+            m.step_handle(it)
+            if active[v]:
+                t0 = time.perf_counter()
+                exp._features(m, x)
+                net.forward(x, y)
+                L.check(exp.lib.pcom_gpu_cnn_apply(m.handle, C.c_void_p(y.data_ptr()), C.byref(stats[v]),
+                                                   float(STEP)), "apply")
+                m.sync()
+                t_net += (time.perf_counter() - t0) / len(runs)
+        if (s + 1) % 6 == 0 or s == steps - 1:
+            for v, m in runs.items():
+                if not active[v]:
+                    continue
+                try:
+                    m.check_finite()
+                except L.PcomError:
+                    m.set_state(**{f: plain.field(f) for f in L.STATE_FIELDS})
+                    active[v] = False
+                    fallback[v] = s + 1
         exp.fine.run(exp.fine_steps)
-    clos.check_finite()
-    res = dict(steps=steps, rms_plain=coarse_rms(exp, plain), rms_closure=coarse_rms(exp, clos),
-               s_per_step_plain=t_plain / steps, s_per_step_closure=t_clos / steps)
-    plain.close()
-    clos.close()
+    res = dict(steps=steps, rms_plain=coarse_rms(exp, plain), s_per_step_plain=t_plain / steps,
+               s_per_step_network=t_net / steps, variants={})
+    for v, m in runs.items():
+        res["variants"][v] = dict(gain=variants[v][0], clip=variants[v][1], rms=coarse_rms(exp, m),
+                                  fell_back_at_step=fallback[v])
+    for m in [plain] + list(runs.values()):
+        m.close()
     return res
 
 
@@ -288,6 +324,8 @@ def main():
     p.add_argument("--spinup-days", type=float, default=2)
     p.add_argument("--train-days", type=float, default=8)
     p.add_argument("--every", type=int, default=2)
+    p.add_argument("--target-steps", type=int, default=1,
+                   help="coarse steps the training residual is accumulated over")
     p.add_argument("--eval-days", type=float, default=2)
     p.add_argument("--epochs", type=int, default=8)
     p.add_argument("--lr", type=float, default=1e-3)
@@ -295,14 +333,14 @@ def main():
     a = p.parse_args()
     torch.cuda.set_device(0)
     t0 = time.time()
-    exp = Experiment(make_case(a.fine), a.factor)
+    exp = Experiment(make_case(a.fine), a.factor, a.target_steps)
     fine_spd = 86400 // exp.fc["dtbc"]
     tf = time.perf_counter()
     exp.fine.run(int(a.spinup_days * fine_spd))
     exp.fine.sync()
     fine_s_per_step = (time.perf_counter() - tf) / max(1, int(a.spinup_days * fine_spd))
     exp.compute_stats()
-    nsamp = int(a.train_days * 24 / a.every)
+    nsamp = int(a.train_days * 24 / max(a.every, a.target_steps))
     xs, ts, mask = exp.generate(nsamp, a.every)
     net = Network(exp.H, exp.W, exp.nk)
     tt = time.perf_counter()
@@ -310,6 +348,7 @@ def main():
     t_train = time.perf_counter() - tt
     ev = evaluate(exp, net, int(a.eval_days * 24))
     res = dict(fine=a.fine, coarse_grid=[exp.W, exp.H, exp.nk], samples=nsamp, epochs=a.epochs,
+               target_steps=a.target_steps,
                train=tr, train_seconds=t_train, eval=ev, stats=exp.stats, fine_s_per_step=fine_s_per_step,
                fine_steps_per_coarse_step=exp.fine_steps, wall_seconds=time.time() - t0)
     line = json.dumps(res)

@@ -184,6 +184,14 @@ __global__ void k_sums_final(const double *part, int nb, double *out) {
   for (int c = 0; c < 3; ++c) out[c] = a[c];
 }
 
+// stream-ordered copy of a Dev (kernel parameter) to device memory
+__global__ void k_copy_dev(const __grid_constant__ Dev P, Dev *out) {
+  const int n = (int)(sizeof(Dev) / sizeof(int));
+  const int *src = reinterpret_cast<const int *>(&P);
+  int *dst = reinterpret_cast<int *>(out);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
 // ---- closure coupling (FP64 handles)
 struct Grid2 {
   int ni, glo_ni, glo_nj, nk;
@@ -217,9 +225,10 @@ __global__ void k_coarsen(const double *f, double *c, const int *levf, Grid2 F, 
   }
 }
 struct CnnStatsDev {
-  float in_mean[5], in_std[5], out_std[4];
+  float in_mean[5], in_std[5], out_std[4], out_gain[4], out_clip;
   double alpha_ref[64];
 };
+__device__ __forceinline__ float clip_y(float y, float c) { return c > 0.f ? fminf(fmaxf(y, -c), c) : y; }
 __global__ void k_cnn_features(const __grid_constant__ Dev P, __nv_bfloat16 *x, CnnStatsDev st) {
   const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
@@ -266,14 +275,16 @@ __global__ void k_cnn_apply(const __grid_constant__ Dev P, const float *y, CnnSt
     const int i = I + 2;
     const long long q2 = (long long)(i - 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
     if (P.lev_u[q2] >= k) {
-      const double du = dt * st.out_std[0] * y[p * 4 + 0], dv = dt * st.out_std[1] * y[p * 4 + 1];
+      const double du = dt * st.out_gain[0] * st.out_std[0] * clip_y(y[p * 4 + 0], st.out_clip);
+      const double dv = dt * st.out_gain[1] * st.out_std[1] * clip_y(y[p * 4 + 1], st.out_clip);
       put_twin(P.uc, G, i, q, P.uc[q] + du);
       put_twin(P.vc, G, i, q, P.vc[q] + dv);
       put_twin(P.up, G, i, q, P.up[q] + du);
       put_twin(P.vp, G, i, q, P.vp[q] + dv);
     }
     if (P.lev_t[q2] >= k) {
-      const double dT = dt * st.out_std[2] * y[p * 4 + 2], dS = dt * st.out_std[3] * y[p * 4 + 3];
+      const double dT = dt * st.out_gain[2] * st.out_std[2] * clip_y(y[p * 4 + 2], st.out_clip);
+      const double dS = dt * st.out_gain[3] * st.out_std[3] * clip_y(y[p * 4 + 3], st.out_clip);
       put_twin(P.tc, G, i, q, P.tc[q] + dT);
       put_twin(P.sc, G, i, q, P.sc[q] + dS);
       if (tp_distinct) {
@@ -324,6 +335,14 @@ struct pcom_handle {
   int n_ts = 0, n_uv = 0, n_w = 0, n_ch = 0, n_ssh = 0;
   int trop_tx = 24, trop_ty = 18, trop_blocks = 0;
   bool trop_resident = false;
+  // domains too large for the resident kernel: the multi-tile kernel over
+  // this domain's tile list (its Dev copied to the device per launch)
+  bool trop_multi = false;
+  int trop_force = 0;  // 0 automatic, 1 resident, 2 multi-tile, 3 generic
+  Dev *d_dev1 = nullptr;
+  TileRef *d_tiles1 = nullptr;
+  int ntiles1 = 0;
+  unsigned long long *d_cnt1 = nullptr;
   unsigned long long trop_epoch = 0;  // barrier arrivals of the barotropic kernel so far
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
@@ -406,7 +425,8 @@ int pick_trop_config(pcom_handle *h) {
   // resident kernel: one tile per CTA, one region point per thread; pick the
   // tiling with the fewest tiles (fewest CTAs at the grid barrier)
   h->trop_resident = false;
-  if (h->D.separable) {
+  h->trop_multi = false;
+  if (h->D.separable && (h->trop_force == 0 || h->trop_force == 1)) {
     int best_n = 1 << 30, bx = 0, by = 0;
     const int mb = trop_fast_max_blocks(24, 18);
     for (int ty = 6; ty <= 40; ++ty)
@@ -421,6 +441,33 @@ int pick_trop_config(pcom_handle *h) {
       h->trop_tx = bx;
       h->trop_ty = by;
       h->trop_blocks = best_n;
+      return PCOM_OK;
+    }
+  }
+  // too large to be resident: the multi-tile kernel (several tiles per CTA,
+  // coefficients from L2) over this domain's tiles
+  if (h->trop_force == 1) return fail(PCOM_ERR_ARG, "the domain does not fit the resident barotropic kernel");
+  if (h->D.separable && (h->trop_force == 0 || h->trop_force == 2)) {
+    const int tx = 32, ty = 8;
+    const int mb = trop_batch_max_blocks(tx, ty);
+    if (mb > 0) {
+      std::vector<TileRef> t;
+      const int G = h->dims.glo_ni, nj = h->nj;
+      for (int j0 = 1; j0 <= nj; j0 += ty)
+        for (int r0 = 0; r0 < G; r0 += tx) t.push_back({0, r0, j0, std::min(tx, G - r0), std::min(ty, nj - j0 + 1)});
+      if (!h->d_dev1) {
+        int rc = h->alloc(&h->d_dev1, 1);
+        if (!rc) rc = h->alloc(&h->d_cnt1, 1);
+        if (rc) return rc;
+      }
+      int rc = h->alloc(&h->d_tiles1, t.size());
+      if (rc) return rc;
+      CK(cudaMemcpy(h->d_tiles1, t.data(), t.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
+      h->ntiles1 = (int)t.size();
+      h->trop_multi = true;
+      h->trop_tx = tx;
+      h->trop_ty = ty;
+      h->trop_blocks = std::min(h->ntiles1, mb);
       return PCOM_OK;
     }
   }
@@ -507,6 +554,12 @@ int do_trop(pcom_handle *h) {
     // the kernel's barrier counter is monotone: pass the arrivals so far
     e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
+  } else if (h->trop_multi) {
+    k_copy_dev<<<1, 256, 0, h->stream>>>(h->D, h->d_dev1);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = launch_trop_batch(h->d_dev1, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1,
+                            h->D.err, h->stream);
   } else {
     e = launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
   }
@@ -1247,6 +1300,8 @@ CnnStatsDev stats_dev(const pcom_cnn_stats *s) {
   memcpy(d.in_mean, s->in_mean, sizeof d.in_mean);
   memcpy(d.in_std, s->in_std, sizeof d.in_std);
   memcpy(d.out_std, s->out_std, sizeof d.out_std);
+  memcpy(d.out_gain, s->out_gain, sizeof d.out_gain);
+  d.out_clip = s->out_clip;
   memcpy(d.alpha_ref, s->alpha_ref, sizeof d.alpha_ref);
   return d;
 }
@@ -1310,6 +1365,14 @@ int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *st,
   k_cnn_apply<<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
   CK(cudaGetLastError());
   h->launches++;
+  return PCOM_OK;
+}
+
+int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which) {
+  if (!h || which < 0 || which > 3) return fail(PCOM_ERR_ARG, "which must be 0..3");
+  CK(cudaStreamSynchronize(h->stream));
+  h->trop_force = which;
+  h->trop_blocks = 0;  // re-pick at the next step
   return PCOM_OK;
 }
 

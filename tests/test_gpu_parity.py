@@ -113,3 +113,20 @@ def test_watchdog_and_errors():
     with pytest.raises(L.PcomError, match="unknown field"):
         L.check(m.lib.pcom_gpu_get_field(m.handle, b"nope", buf.ctypes.data_as(L.dbl_p), 4), "get_field")
     m.close()
+
+
+@pytest.mark.parametrize("which", [2, 3])
+def test_barotropic_kernel_forms(oracle_lib, which):
+    """The multi-tile (2) and generic (3) barotropic kernels, forced on a
+    domain the resident kernel would take, give the oracle's result too."""
+    from pcom_b200 import _lib as L
+
+    c = make_case("tiny_bathy")
+    o = oracle_lib.Oracle(c)
+    m = Model(c)
+    L.check(m.lib.pcom_gpu_set_trop_kernel(m.handle, which), "set_trop_kernel")
+    lev_t = m.static()["lev_t"]
+    m.run(5)
+    o.step(5)
+    _check(m, o, STATE_FIELDS, lev_t, c["nk"], f"barotropic kernel {which} after 5 steps")
+    m.close()
