@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__res
     for (int q = tid; q < kM * KC; q += kThreads) {
       const int m = q / KC, c = q % KC;
       const long long p = p0 + m;
-      const long long src = p < npix ? tap_src(p, t, H, W, periodic_x) : -1;
+      long long src = p < npix ? tap_src(p, t, H, W, periodic_x) : -1;
+      if (src >= npix) src = -1;  // a partial last image: missing pixels are zero
       const uint32_t dst = smem_u32(A) + (uint32_t)(((m / 8) * KC + c) * 128 + (m % 8) * 16);
       cp_async16(dst, src >= 0 ? (const void *)(in + src * CIN + c * 8) : (const void *)in, src >= 0);
     }
@@ -244,6 +245,182 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__res
 }
 
 // ----------------------------------------------------------------------------
+// Persistent form of the same convolution.  A tile is 128 consecutive pixels
+// of one image row; its 3 x 130 halo of input pixels is loaded once into
+// shared memory "chunk-planar" (plane c holds channels 8c..8c+7 of every
+// halo pixel, 16 bytes per pixel, pixels contiguous), so that the A operand
+// of tap (dy, dx) is the same planes read from a start address shifted by
+// (dy + 1) * 130 + (dx + 1) pixels: leading byte offset = plane size (K
+// direction), stride byte offset = 128 bytes (8 pixels).  All 9 taps of the
+// weights stay in shared memory for the kernel's lifetime; the next tile's
+// halo loads while the tensor cores work on the current one.
+constexpr int kHaloW = kM + 2;                 // halo columns
+constexpr int kPlane = 3 * kHaloW * 16;        // bytes per 8-channel plane
+
+template <int CIN, int NOUT>
+__global__ void __launch_bounds__(kThreads) k_conv_halo(const __nv_bfloat16 *__restrict__ in,
+                                                        const __nv_bfloat16 *__restrict__ w,
+                                                        const float *__restrict__ bias,
+                                                        const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
+                                                        int H, int W, int periodic_x, int mode, int nstore, int *err) {
+  constexpr int KC = CIN / 8;
+  constexpr int W_BYTES = 9 * NOUT * CIN * 2;
+  constexpr int A_BYTES = KC * kPlane;
+  constexpr int ROWB = NOUT * 2 + 16;  // padded BF16 row of the output staging tile
+  constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  uint8_t *Wsm = smem, *Abuf[2] = {smem + W_BYTES, smem + W_BYTES + A_BYTES};
+  uint8_t *Osm = smem + W_BYTES + 2 * A_BYTES;  // kM rows of ROWB bytes
+  const int ntx = (W + kM - 1) / kM;
+  const long long ntiles = (long long)nimg * H * ntx;
+
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), NCOLS);
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // weights: tap t, core matrix (n/8, c) at t*NOUT*CIN*2 + ((n/8)*KC + c)*128 + (n%8)*16
+  for (int q = tid; q < 9 * NOUT * KC; q += kThreads) {
+    const int t = q / (NOUT * KC), r = q % (NOUT * KC), n = r / KC, c = r % KC;
+    const uint32_t dst = smem_u32(Wsm) + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16);
+    cp_async16(dst, w + ((long long)t * NOUT + n) * CIN + c * 8, true);
+  }
+  auto load_halo = [&](long long tile, uint8_t *A) {
+    const int tx = (int)(tile % ntx);
+    const long long row = tile / ntx;  // img * H + y
+    const int y = (int)(row % H);
+    const long long img = row / H;
+    const int x0 = tx * kM;
+    for (int q = tid; q < 3 * kHaloW * KC; q += kThreads) {
+      const int pix = q / KC, c = q % KC, r = pix / kHaloW, u = pix % kHaloW;
+      const int yy = y + r - 1;
+      int xx = x0 - 1 + u;
+      bool ok = yy >= 0 && yy < H;
+      if (xx < 0 || xx >= W) {
+        if (periodic_x) xx = ((xx % W) + W) % W;
+        else ok = false;
+      }
+      const long long src = (img * H + yy) * W + xx;
+      const uint32_t dst = smem_u32(A) + (uint32_t)(c * kPlane + pix * 16);
+      cp_async16(dst, ok ? (const void *)(in + src * CIN + c * 8) : (const void *)in, ok);
+    }
+  };
+  long long tile = blockIdx.x;
+  if (tile < ntiles) load_halo(tile, Abuf[0]);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
+    uint8_t *A = Abuf[it & 1];
+    cp_async_wait_all();  // this tile's halo (and, the first time, the weights)
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      #pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        #pragma unroll
+        for (int j = 0; j < CIN / 16; ++j) {
+          const uint32_t a0 = smem_u32(A) + (uint32_t)(((t / 3) * kHaloW + (t % 3)) * 16 + 2 * j * kPlane);
+          const uint64_t ad = umma_desc(a0, kPlane, 128);
+          const uint64_t bd = umma_desc(smem_u32(Wsm) + (uint32_t)(t * NOUT * CIN * 2 + j * 256), 128, KC * 128);
+          umma_bf16(tmem, ad, bd, idesc, (t > 0 || j > 0) ? 1u : 0u);
+        }
+      }
+      umma_commit(smem_u32(&mbar));
+    }
+    // the next tile's halo goes to the other buffer (its last readers, the
+    // previous tile's MMAs, have completed)
+    const long long next = tile + gridDim.x;
+    if (next < ntiles) load_halo(next, Abuf[(it + 1) & 1]);
+    if (!mbar_wait(smem_u32(&mbar), phase)) {
+      ok = false;
+      if (tid == 0) atomicExch(err, 1);
+      mbar_wait(smem_u32(&mbar), phase);  // one more bounded wait for the MMAs in flight
+      break;
+    }
+    phase ^= 1;
+    tc_fence_after();
+    const int tx = (int)(tile % ntx);
+    const long long row = tile / ntx;
+    const int m = warp * 32 + lane, x0 = tx * kM, x = x0 + m;
+    const int nvalid = min(kM, W - x0);
+    const long long p = row * W + x;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    if (mode == 2) {
+      // the tile's ReLU mask rows, coalesced, into the staging tile
+      const uint4 *src = reinterpret_cast<const uint4 *>(aux + (row * W + x0) * NOUT);
+      for (int q = tid; q < nvalid * (NOUT / 8); q += kThreads)
+        *reinterpret_cast<uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16) = src[q];
+      __syncthreads();
+    }
+    #pragma unroll
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      float v[16];
+      tmem_ld16(lane_addr + c0, v);
+      if (mode == 1) {
+        if (x < W && c0 == 0) {
+          float *o = (float *)out + p * nstore;
+          if (nstore == 4) {
+            *reinterpret_cast<float4 *>(o) =
+                make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
+          } else {
+            for (int q = 0; q < 16 && q < nstore; ++q) o[q] = v[q] + bias[q];
+          }
+        } else if (x < W) {
+          float *o = (float *)out + p * nstore;
+          for (int q = 0; q < 16; ++q)
+            if (c0 + q < nstore) o[c0 + q] = v[q] + bias[c0 + q];
+        }
+      } else {
+        uint4 *srow = reinterpret_cast<uint4 *>(Osm + m * ROWB + c0 * 2);
+        uint32_t pk[8];
+        if (mode == 0) {
+          #pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v[2 * q] + bias[c0 + 2 * q], 0.f),
+                                                            fmaxf(v[2 * q + 1] + bias[c0 + 2 * q + 1], 0.f));
+            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+          }
+        } else {
+          const uint4 a0 = srow[0], a1 = srow[1];
+          const uint32_t aw[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+          #pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw[q]);
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(__low2float(a2) > 0.f ? v[2 * q] : 0.f,
+                                                            __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f);
+            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+          }
+        }
+        srow[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        srow[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+      }
+    }
+    if (mode != 1) {
+      __syncthreads();
+      // the tile's output rows are contiguous in global memory
+      uint4 *dst = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (row * W + x0) * NOUT);
+      for (int q = tid; q < nvalid * (NOUT / 8); q += kThreads)
+        dst[q] = *reinterpret_cast<const uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16);
+    }
+    tc_fence_before();
+    __syncthreads();  // accumulator and staging tile read before the next tile
+  }
+  cp_async_wait_all();
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+}
+
+// ----------------------------------------------------------------------------
 // Weight gradient: dw[t][n][c] += sum_p in[src(p, t)][c] g[p][n]
 // Tile rows r = (t - t0) * CIN + c for TPT = 128 / CIN taps starting at
 // t0 = blockIdx.y * TPT; K = pixels, 64 per stage; CTA x covers ppc pixels.
@@ -296,7 +473,8 @@ __global__ void __launch_bounds__(kThreads) k_wgrad_tc(const __nv_bfloat16 *__re
       const int g = q / KP, k = q % KP;
       const int r0 = g * 8, t = t0 + r0 / CIN, c = r0 % CIN;
       const long long p = pk + k;
-      const long long src = (t < 9 && p < pend) ? tap_src(p, t, H, W, periodic_x) : -1;
+      long long src = (t < 9 && p < pend) ? tap_src(p, t, H, W, periodic_x) : -1;
+      if (src >= npix) src = -1;
       const uint32_t dst = smem_u32(A) + (uint32_t)((g * KG + k / 8) * 128 + (k % 8) * 16);
       cp_async16(dst, src >= 0 ? (const void *)(in + src * CIN + c) : (const void *)in, src >= 0);
     }
@@ -358,9 +536,39 @@ template <int CIN, int NOUT>
 size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 64 * 2)); }
 
 template <int CIN, int NOUT>
+size_t halo_smem() {
+  return smem_floor<NOUT>((size_t)9 * NOUT * CIN * 2 + 2 * (size_t)(CIN / 8) * kPlane + (size_t)kM * (NOUT * 2 + 16));
+}
+
+template <int CIN, int NOUT>
+cudaError_t conv_halo_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                             const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x, int mode,
+                             int nstore, int *err, cudaStream_t s) {
+  const size_t sm = halo_smem<CIN, NOUT>();
+  cudaError_t e = cudaFuncSetAttribute(k_conv_halo<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const long long hw = (long long)H * W;
+  const int nimg = (int)(npix / hw);
+  const long long ntiles = (long long)nimg * H * ((W + kM - 1) / kM);
+  int dev = 0, nsm = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_halo<CIN, NOUT>, kThreads, sm);
+  const int tmem_cap = 512 / (NOUT < 32 ? 32 : NOUT);
+  per = per < 1 ? 1 : (per > tmem_cap ? tmem_cap : per);
+  const long long grid = ntiles < (long long)nsm * per ? ntiles : (long long)nsm * per;
+  k_conv_halo<CIN, NOUT><<<(unsigned)grid, kThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
+                                                              nstore, err);
+  return cudaGetLastError();
+}
+
+template <int CIN, int NOUT>
 cudaError_t conv_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, const __nv_bfloat16 *aux,
                         void *out, long long npix, int H, int W, int periodic_x, int mode, int nstore, int *err,
                         cudaStream_t s) {
+  // whole images: the persistent halo form
+  if (npix % ((long long)H * W) == 0)
+    return conv_halo_launch<CIN, NOUT>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
   const size_t sm = conv_smem<CIN, NOUT>();
   cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;

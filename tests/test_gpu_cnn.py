@@ -61,6 +61,29 @@ def test_conv_layer(cin, nout, mode, px):
         assert np.abs(got - ref).max() <= 2 ** -8 * scale + 1e-6
 
 
+@pytest.mark.parametrize("cin,nout", [(16, 64), (64, 64), (64, 16)])
+def test_conv_partial_image(cin, nout):
+    """A pixel count that is not whole images takes the per-tap tile form."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    npix = H * W * NIMG - 37
+    xd, x = bf16(rng.standard_normal((npix, cin)))
+    wd, w = bf16(rng.standard_normal((9, nout, cin)) / np.sqrt(9 * cin))
+    b = rng.standard_normal(nout).astype(np.float32)
+    bd = torch.from_numpy(b).cuda()
+    outd = torch.zeros((npix, 4), dtype=torch.float32, device="cuda")
+    rc = L.load().pcom_cnn_conv_layer(cin, nout, xd.data_ptr(), wd.data_ptr(), bd.data_ptr(), None, outd.data_ptr(),
+                                      npix, H, W, 1, 1, 4, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    cnn_check(rc, "conv")
+    # the oracle on whole images, restricted to the pixels computed (the last
+    # image is partial: its missing pixels are zero input)
+    full = np.zeros((H * W * NIMG, cin), np.float32)
+    full[:npix] = x
+    ref = pycnn.conv(cin, nout, full, w, b, None, H, W, 1, 1, 4)[:npix]
+    assert np.abs(outd.cpu().numpy() - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("px", [0, 1])
 @pytest.mark.parametrize("cin,nout", [(16, 64), (64, 64), (64, 16)])
 def test_wgrad(cin, nout, px):
