@@ -68,6 +68,7 @@ def parse():
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    p.add_argument("--no-closure", action="store_true", help="skip the closure-network leg")
     p.add_argument("--workload", default="global1", choices=["global1", "ensemble"],
                    help="ensemble: 32 perturbed 1-degree members + 16 uneven basins, batched")
     p.add_argument("--members", type=int, default=32)
@@ -289,6 +290,9 @@ def run_ours(args):
     mixed = None
     if not args.no_mixed:
         mixed = run_mixed_leg(args, case, stream, steps)
+    closure = None
+    if not args.no_closure:
+        closure = run_closure_leg(args, case, ms_per_step)
 
     # ------------------------------------------------ CPU baseline (rank 0, N = 1)
     cpu = None
@@ -329,6 +333,7 @@ def run_ours(args):
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "cpu_baseline": cpu,
             "mixed": mixed,
+            "closure": closure,
         }
         print(json.dumps(line))
     m.close()
@@ -378,6 +383,83 @@ def run_mixed_leg(args, case, stream, steps):
     b.close()
     return {"ms_per_step": round(ms, 4), "value": round(sypd(ms / 1000.0), 2), "unit": "SYPD", "dtype": "f32 stencils, f64 barotropic",
             "rel_rms_error_vs_fp64_after_24_steps": {k_: float(f"{v:.3e}") for k_, v in err.items()}}
+
+
+def run_closure_leg(args, case, plain_ms):
+    """Cost of the closure form on the same grid: per step the network's
+    input features, its forward pass (5 tcgen05 convolutions over the 30
+    level images) and the tendency application, timed with CUDA events after
+    the plain step; tensor throughput against the measured BF16 peak.  The
+    weights are random here (cost does not depend on them); the closure's
+    accuracy is measured by pcom_b200.closure against the coarse-grained
+    0.25-degree run."""
+    import ctypes as C
+
+    import torch
+
+    from pcom_b200 import _lib as L
+    from pcom_b200.closure import Network
+    from pcom_b200.model import Model
+
+    m = Model(case)
+    m.run(2)
+    H, W, nk = case["glo_nj"], case["glo_ni"], case["nk"]
+    npix = H * W * nk
+    net = Network(H, W, nk, seed=3)
+    x = torch.zeros((npix, 16), dtype=torch.bfloat16, device="cuda")
+    y = torch.zeros((npix, 4), dtype=torch.float32, device="cuda")
+    st = L.CnnStats()
+    for q in range(5):
+        st.in_std[q] = 1.0
+    for q in range(4):
+        st.out_std[q] = 1e-9
+        st.out_gain[q] = 1.0
+    st.out_clip = 3.0
+    stream = torch.cuda.current_stream()
+    m.set_stream(stream.cuda_stream)
+    net.set_stream(stream.cuda_stream)
+    lib = m.lib
+
+    def once():
+        L.check(lib.pcom_gpu_cnn_features(m.handle, C.c_void_p(x.data_ptr()), C.byref(st)), "features")
+        net.forward(x, y)
+        L.check(lib.pcom_gpu_cnn_apply(m.handle, C.c_void_p(y.data_ptr()), C.byref(st), 3600.0), "apply")
+
+    for _ in range(3):
+        once()
+    torch.cuda.synchronize()
+    n = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n):
+        once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    net_ms = e0.elapsed_time(e1) / n
+    # the forward alone, for the tensor-core throughput
+    e0.record(stream)
+    for _ in range(n):
+        net.forward(x, y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / n
+    flop = npix * 9 * 2 * (16 * 64 + 3 * 64 * 64 + 64 * 16)  # padded channels, as issued
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    tf = flop / (fwd_ms * 1e-3) / 1e12
+    net.close()
+    m.close()
+    total = plain_ms + net_ms
+    return {"ms_per_step": round(total, 4), "network_ms_per_step": round(net_ms, 4), "value": round(sypd(total / 1000.0), 2),
+            "unit": "SYPD", "forward_ms": round(fwd_ms, 4),
+            "tensor": {"achieved": round(tf, 1), "peak": peak, "unit": "TFLOP/s",
+                       "peak_source": "measured" if "bf16_tflops" in peaks else "fallback",
+                       "frac": round(tf / peak, 4), "flop_per_forward": flop},
+            "note": "cost of the closure form on this grid with random weights; accuracy: pcom_b200.closure"}
 
 
 def ensemble_cases(members: int, basins: int, member_case: str = "box"):
