@@ -25,7 +25,7 @@ typedef struct pcom_case {
   int32_t glo_ni, glo_nj, nk;
   int32_t dtbt, dtbc;             /* namelist time_ctrl dtbt, dtbc */
   int32_t r8;                     /* 1: literals as REAL(8) (ifort -r8) */
-  int32_t rst;                    /* namelist restart_run (0 supported here) */
+  int32_t rst;                    /* namelist restart_run: 1 = the caller loads a restart state after create */
   int32_t year, month, day, hour; /* namelist bdate */
   const double *lon, *lat, *z, *tmn, *smn; /* initial.nc: lon (glo_ni), lat (glo_nj), z/tmn/smn (nk) */
   const int32_t *itn;                      /* initial.nc itn: glo_ni*glo_nj */

@@ -375,7 +375,9 @@ extern "C" {
 
 int pcom_model_create(const pcom_case *c, int32_t flags, pcom_model **out) {
   if (!c || !out) return PCOM_ERR_ARG;
-  if (c->rst != 0) return PCOM_ERR_ARG;  // restart input is read by the Fortran driver, not here
+  // rst = 1: the setup is the same; the caller then loads the restart state
+  // (pcom_gpu_set_state) and the AB3 start-up is skipped (mod_int.f90:122-132)
+  if (c->rst != 0 && c->rst != 1) return PCOM_ERR_ARG;
   pcom_model *M = new pcom_model();
   M->r8 = c->r8 != 0;
   M->glo_ni = c->glo_ni; M->glo_nj = c->glo_nj; M->nk = c->nk;

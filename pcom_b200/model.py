@@ -153,6 +153,9 @@ class Model:
         out.update(n_ts=a.n_ts, n_uv=a.n_uv, n_w=a.n_w, n_ch=a.n_ch, n_ssh=a.n_ssh)
         return out
 
+    def reset_accum(self):
+        L.check(self.lib.pcom_gpu_reset_accum(self.handle), "reset_accum")
+
     def set_state(self, **fields):
         keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in fields.items()}
         st = L.State(*[(_dp(keep[n]) if n in keep else None) for n in L.STATE_FIELDS])
