@@ -155,6 +155,14 @@ int64_t pcom_gpu_field_size(pcom_handle *h, const char *name);
 /* Run the NaN/Inf watchdog over the prognostic fields; PCOM_ERR_NUMERIC if
  * any wet point is not finite. */
 int pcom_gpu_check_finite(pcom_handle *h);
+/* Daily forcing on the device (int_bnd, mod_int.f90:649-691): upload the 12
+ * monthly fields once (each pointer: 12 x ni x nj doubles, month slowest,
+ * the layout of frc%*%v; fw is not used by the step and may be NULL), then
+ * per model day bnd = (frc(m2) - frc(m1)) f + frc(m1) with the months and
+ * weight int_bnd computes from the calendar.  Replaces the daily host
+ * int_bnd + pcom_gpu_set_forcing upload. */
+int pcom_gpu_set_forcing_months(pcom_handle *h, const pcom_forcing *months);
+int pcom_gpu_int_bnd(pcom_handle *h, int32_t m1, int32_t m2, double f);
 /* Barotropic kernel choice: 0 automatic (resident when the domain's tiles
  * fit one per CTA, else multi-tile), 1 resident (one region point per
  * thread, coefficients in registers), 2 multi-tile (several tiles per CTA),

@@ -184,6 +184,19 @@ __global__ void k_sums_final(const double *part, int nb, double *out) {
   for (int c = 0; c < 3; ++c) out[c] = a[c];
 }
 
+// int_bnd (mod_int.f90:649-691): bnd = (frc(m2) - frc(m1)) f + frc(m1)
+__global__ void k_int_bnd(const double *frc, double *taux, double *tauy, double *t, double *s, double *pa,
+                          long long n2, int m1, int m2, double f) {
+  double *dst[5] = {taux, tauy, t, s, pa};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < 5 * n2; p += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(p / n2);
+    const long long r = p % n2;
+    const double *F = frc + (long long)q * 12 * n2;
+    const double a = F[(long long)(m1 - 1) * n2 + r], b = F[(long long)(m2 - 1) * n2 + r];
+    dst[q][r] = (b - a) * f + a;
+  }
+}
+
 // stream-ordered copy of a Dev (kernel parameter) to device memory
 __global__ void k_copy_dev(const __grid_constant__ Dev P, Dev *out) {
   const int n = (int)(sizeof(Dev) / sizeof(int));
@@ -343,6 +356,7 @@ struct pcom_handle {
   TileRef *d_tiles1 = nullptr;
   int ntiles1 = 0;
   unsigned long long *d_cnt1 = nullptr;
+  double *frc_months = nullptr;  // taux, tauy, t, s, pa: [5][12][nj][ni]
   unsigned long long trop_epoch = 0;  // barrier arrivals of the barotropic kernel so far
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
@@ -1363,6 +1377,34 @@ int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *st,
   if (!h || !y || !st) return fail(PCOM_ERR_ARG, "null argument");
   if (h->mixed) return fail(PCOM_ERR_ARG, "the closure is applied on FP64 handles");
   k_cnn_apply<<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
+  CK(cudaGetLastError());
+  h->launches++;
+  return PCOM_OK;
+}
+
+int pcom_gpu_set_forcing_months(pcom_handle *h, const pcom_forcing *months) {
+  if (!h || !months) return fail(PCOM_ERR_ARG, "null argument");
+  const long long n2 = h->n2;
+  if (!h->frc_months) {
+    int rc = h->alloc(&h->frc_months, (size_t)(5 * 12 * n2));
+    if (rc) return rc;
+  }
+  const double *src[5] = {months->taux, months->tauy, months->t, months->s, months->pa};
+  for (int q = 0; q < 5; ++q) {
+    if (!src[q]) return fail(PCOM_ERR_ARG, "monthly forcing field %d missing", q);
+    CK(cudaMemcpyAsync(h->frc_months + (long long)q * 12 * n2, src[q], 12 * n2 * sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream));
+  }
+  return sync_check(h);
+}
+
+int pcom_gpu_int_bnd(pcom_handle *h, int32_t m1, int32_t m2, double f) {
+  if (!h) return fail(PCOM_ERR_ARG, "null handle");
+  if (!h->frc_months) return fail(PCOM_ERR_STATE, "pcom_gpu_int_bnd before pcom_gpu_set_forcing_months");
+  if (m1 < 1 || m1 > 12 || m2 < 1 || m2 > 12) return fail(PCOM_ERR_ARG, "months must be 1..12");
+  Dev &D = h->D;
+  k_int_bnd<<<256, 256, 0, h->stream>>>(h->frc_months, (double *)D.taux, (double *)D.tauy, (double *)D.bnd_t,
+                                        (double *)D.bnd_s, (double *)D.bnd_pa, h->n2, m1, m2, f);
   CK(cudaGetLastError());
   h->launches++;
   return PCOM_OK;

@@ -345,10 +345,9 @@ void setup(pcom_model &M, const pcom_case &c) {
 }
 
 // int_bnd (mod_int.f90:649-691): monthly forcing interpolated to the day
-void int_bnd(pcom_model &M) {
+// the months and weight of int_bnd (mod_int.f90:649-691) at the model date
+void bnd_weights(const pcom_model &M, int &m1, int &m2, double &f) {
   const int y = M.ct.y, m = M.ct.m, d = M.ct.d;
-  int m1, m2;
-  double f;
   if (d < 15) {
     m2 = m;
     m1 = (m == 1) ? 12 : m - 1;
@@ -361,6 +360,12 @@ void int_bnd(pcom_model &M) {
     const int days = month_days(y, m1);
     f = M.r8 ? (d - 15.0) / (days - 15 + 15.0) : (double)(((float)d - 15.0f) / ((float)(days - 15) + 15.0f));
   }
+}
+
+void int_bnd(pcom_model &M) {
+  int m1, m2;
+  double f;
+  bnd_weights(M, m1, m2, f);
   for (int q = 0; q < 6; ++q)
     for (int j = 1; j <= M.nj; ++j)
       for (int i = 1; i <= M.ni; ++i)
@@ -402,6 +407,12 @@ int pcom_model_create(const pcom_case *c, int32_t flags, pcom_model **out) {
     st.tc = M->t0.v.data(); st.sc = M->s0.v.data();
     rc = pcom_gpu_set_state(M->h, &st);
   }
+  if (!rc) {
+    // the 12 monthly forcing fields, for int_bnd on the device
+    pcom_forcing mo{M->frc[0].v.data(), M->frc[1].v.data(), M->frc[2].v.data(),
+                    M->frc[3].v.data(), M->frc[4].v.data(), M->frc[5].v.data()};
+    rc = pcom_gpu_set_forcing_months(M->h, &mo);
+  }
   if (rc) { pcom_gpu_destroy(M->h); delete M; return rc; }
   *out = M;
   return PCOM_OK;
@@ -422,11 +433,12 @@ int pcom_model_run(pcom_model *M, int64_t nsteps) {
   for (int64_t n = 0; n < nsteps; ++n) {
     M->iter += 1;
     if (M->iter == 1 || M->ct.d != M->pt.d) {
-      int_bnd(*M);
+      // int_bnd on the device from the monthly fields uploaded at create
+      int m1, m2;
+      double f;
+      bnd_weights(*M, m1, m2, f);
       M->nday += 1;
-      pcom_forcing f{M->bnd[0].v.data(), M->bnd[1].v.data(), M->bnd[2].v.data(),
-                     M->bnd[3].v.data(), M->bnd[4].v.data(), M->bnd[5].v.data()};
-      int rc = pcom_gpu_set_forcing(M->h, &f);
+      int rc = pcom_gpu_int_bnd(M->h, m1, m2, f);
       if (!rc) rc = pcom_gpu_den_prho(M->h);
       if (rc) return rc;
     }
@@ -458,11 +470,11 @@ int pcom_model_run_batch(pcom_model *const *ms, int32_t n, pcom_batch *b, int64_
       pcom_model &M = *ms[m];
       M.iter += 1;
       if (day) {
-        int_bnd(M);
+        int m1, m2;
+        double f;
+        bnd_weights(M, m1, m2, f);
         M.nday += 1;
-        pcom_forcing f{M.bnd[0].v.data(), M.bnd[1].v.data(), M.bnd[2].v.data(),
-                       M.bnd[3].v.data(), M.bnd[4].v.data(), M.bnd[5].v.data()};
-        int rc = pcom_gpu_set_forcing(M.h, &f);
+        int rc = pcom_gpu_int_bnd(M.h, m1, m2, f);
         if (rc) return rc;
       }
     }

@@ -130,3 +130,18 @@ def test_barotropic_kernel_forms(oracle_lib, which):
     o.step(5)
     _check(m, o, STATE_FIELDS, lev_t, c["nk"], f"barotropic kernel {which} after 5 steps")
     m.close()
+
+
+def test_device_int_bnd_matches_host():
+    """The daily forcing interpolated on the device (pcom_gpu_int_bnd, used
+    by the time loop) equals the host int_bnd (mod_int.f90:649-691) bitwise."""
+    c = make_case("tiny_bathy")
+    # distinct months, so the interpolation weight matters
+    for k in ("taux", "bct"):
+        c[k] = c[k] * (1.0 + 0.1 * np.arange(12))[:, None, None]
+    m = Model(c)
+    m.run(25)  # over the first day boundary: int_bnd ran for day 2
+    host = m.int_bnd()
+    for name, key in (("bnd_taux", "taux"), ("bnd_t", "t"), ("bnd_s", "s"), ("bnd_tauy", "tauy")):
+        assert np.array_equal(m.field(name), host[key]), name
+    m.close()
