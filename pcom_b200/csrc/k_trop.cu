@@ -683,6 +683,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     k_trop_fast(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, const TileRef *__restrict__ tiles,
                 int TX, int TY, int ntx, unsigned long long epoch, unsigned long long *gcnt, int *gerr) {
   extern __shared__ double sm[];
+  __shared__ int s_stop;
   const TileRef T = GROUP ? tiles[blockIdx.x] : TileRef{0, 0, 0, 0, 0};
   const Dev &P = GROUP ? Ps[T.m] : P0;
   unsigned long long *const bar_cnt = GROUP ? gcnt : P.tile_flag;
@@ -922,27 +923,31 @@ __global__ void __launch_bounds__(kResThreads, 1)
       acc_u = acc_u + ubc;
       acc_v = acc_v + vbc;
     }
-    // grid barrier on a monotone arrival counter: each CTA adds 1 after
-    // making its writes visible, then waits (bounded) for all arrivals of
-    // this substep; the counter is never reset, targets grow per launch
+    // grid barrier on a monotone arrival counter: after the CTA barrier,
+    // thread 0 adds 1 with release semantics (cumulative over the CTA's
+    // writes ordered before it by bar.sync), then waits (bounded, acquire)
+    // for all arrivals of this substep; the counter is never reset, targets
+    // grow per launch.  The outcome reaches the CTA through shared memory.
     __syncthreads();
     if (tid == 0) {
-      __threadfence();
-      atomicAdd(bar_cnt, 1ULL);
-      const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*bar_cnt);
       cuda::atomic_ref<int, cuda::thread_scope_device> err(bar_err[0]);
+      c.fetch_add(1ULL, cuda::memory_order_release);
+      const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
       long long it = 0;
+      int stop = 0;
       while (c.load(cuda::memory_order_acquire) < want) {
         if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
           err.store(1, cuda::memory_order_relaxed);
+          stop = 1;
           break;
         }
         if (it > 1024) __nanosleep(32);
       }
+      s_stop = stop;
     }
     __syncthreads();
-    if (*(volatile int *)bar_err != 0) return;
+    if (s_stop) return;
   }
   if (inS8) {
     const double ub = acc_u / (nstep + 1), vb = acc_v / (nstep + 1);

@@ -31,10 +31,10 @@ __device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, 
   __syncthreads();
   __shared__ int s_fail;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(cnt, 1ULL);
+    // release: cumulative over the CTA's writes ordered before it by bar.sync
     cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*cnt);
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    c.fetch_add(1ULL, cuda::memory_order_release);
     long long it = 0;
     int f = 0;
     while (c.load(cuda::memory_order_acquire) < want) {
