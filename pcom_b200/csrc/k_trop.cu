@@ -784,8 +784,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
     const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
     const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
-    // S1: previous state
-    if (active) {  // L2 loads (.cg): the buffers were written by other SMs
+    // S1: previous state.  After the first substep the tile's own points
+    // already hold it (written in S8), so only the 2-cell ring comes from
+    // L2 (.cg loads: written by other SMs)
+    if (active && (nt == 1 || !inS8)) {
       S(R_CH, p) = __ldcg(src_ch + q);
       if (inS2) { S(R_UB, p) = __ldcg(src_ub + q); S(R_VB, p) = __ldcg(src_vb + q); }
     }
@@ -918,6 +920,11 @@ __global__ void __launch_bounds__(kResThreads, 1)
       st2(P.tr_ch[d2], P, i, q, chn);
       st2(P.tr_ub[d2], P, i, q, ubc);
       st2(P.tr_vb[d2], P, i, q, vbc);
+      // the next substep's state at this point (during S8 only this thread
+      // reads these three entries)
+      S(R_CH, p) = chn;
+      S(R_UB, p) = ubc;
+      S(R_VB, p) = vbc;
       if (nt <= nstep / 2) acc_m = acc_m + chn;
       acc_m2 = acc_m2 + chn;
       acc_u = acc_u + ubc;
