@@ -192,7 +192,7 @@ int64_t pcom_gpu_launch_count(pcom_handle *h);
  * subgrid closure (include/pcom_cnn.h) on FP64 handles. */
 typedef struct {
   float in_mean[5], in_std[5];  /* u, v, T, S, alpha - alpha_ref(k) */
-  float out_std[4];             /* du, dv, dT, dS tendency scales */
+  float out_std[4];             /* du, dv, dT, dS tendency scales (0: output unused) */
   float out_gain[4];            /* applied fraction per output (pcom_gpu_cnn_apply) */
   float out_clip;               /* |y| limit in units of out_std (0: none) */
   double alpha_ref[64];         /* [k - 1], k = 1..nk */
@@ -200,7 +200,8 @@ typedef struct {
 /* Set the coarse handle's state to the block means (factor x factor) of the
  * fine handle's state over wet fine cells: T-grid fields (tc, sc, tp, sp,
  * ch, mch, mch2) on T cells, U-grid fields (uc, vc, up, vp, the AB3
- * history, am, ub, vb) on U points.  The grids must nest: fine glo_ni,
+ * history, am, ub, vb) on U points, velocities and their history set to 0
+ * where the coarse U point is land.  The grids must nest: fine glo_ni,
  * glo_nj = factor x coarse, and the coarse levels no deeper than any fine
  * column of their block. */
 int pcom_gpu_coarsen(pcom_handle *fine, pcom_handle *coarse, int32_t factor);

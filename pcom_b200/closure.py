@@ -154,11 +154,17 @@ class Experiment:
         L.check(self.lib.pcom_gpu_cnn_features(m.handle, C.c_void_p(x.data_ptr()), C.byref(self.st)), "features")
         m.sync()
 
+    def _current_alpha(self, m: Model):
+        """den_alpha of the model's current T, S, ch (alpha is not carried
+        over by coarse-graining)."""
+        m.phase("den_alpha", self.citer)
+
     def compute_stats(self):
         """Input normalisation from the current coarse-grained fine state and
         output scales from one target sample."""
         torch = self.torch
         self.coarsen(self.pred)
+        self._current_alpha(self.pred)
         st = self.pred.static()
         k = np.arange(1, self.nk + 1)[:, None, None]
         wt, wu = st["lev_t"][None] >= k, st["lev_u"][None] >= k
@@ -176,7 +182,9 @@ class Experiment:
         mk = torch.zeros((self.npix, 4), dtype=torch.float32, device="cuda")
         self._one_target(t, mk)
         tn, mn = t.cpu().numpy(), mk.cpu().numpy()
-        self.stats["out_std"] = [float(np.sqrt((tn[:, q] ** 2 * mn[:, q]).sum() / max(mn[:, q].sum(), 1))) or 1.0
+        # a residual that is identically zero (e.g. S of a case with uniform
+        # salinity) gets scale 0: its target is 0 and the closure never adds it
+        self.stats["out_std"] = [float(np.sqrt((tn[:, q] ** 2 * mn[:, q]).sum() / max(mn[:, q].sum(), 1)))
                                  for q in range(4)]
         self.st = _stats_struct(self.stats)
 
@@ -188,6 +196,7 @@ class Experiment:
         self.coarsen(self.pred)
         self.pred.den_prho()
         if x is not None:
+            self._current_alpha(self.pred)
             self._features(self.pred, x)
         for _ in range(self.kt):
             self.citer += 1
@@ -248,6 +257,7 @@ VARIANTS = {  # applied fraction of each output (du, dv, dT, dS) and the |y| cli
     "all": ([1.0, 1.0, 1.0, 1.0], 3.0),
     "tracers": ([0.0, 0.0, 1.0, 1.0], 3.0),
     "tracers+0.25uv": ([0.25, 0.25, 1.0, 1.0], 3.0),
+    "tracers-half": ([0.0, 0.0, 0.5, 0.5], 3.0),
 }
 
 

@@ -216,8 +216,10 @@ __device__ __forceinline__ void put_twin(double *f, const Grid2 &g, int i, long 
   else if (i == g.ni - 1) f[q - (g.ni - 2)] = v;
 }
 // block mean over wet fine cells (all cells when none is wet) of nlev planes
-__global__ void k_coarsen(const double *f, double *c, const int *levf, Grid2 F, Grid2 Cg, int nlev, int factor,
-                          int plane_lev) {
+// levc (optional): the coarse grid's levels; the value is 0 where the
+// coarse point is land (U-grid velocities must vanish there)
+__global__ void k_coarsen(const double *f, double *c, const int *levf, const int *levc, Grid2 F, Grid2 Cg, int nlev,
+                          int factor, int plane_lev) {
   const long long n = (long long)Cg.glo_ni * Cg.glo_nj * nlev;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
     const int I = (int)(p % Cg.glo_ni), J = (int)((p / Cg.glo_ni) % Cg.glo_nj), k = (int)(p / ((long long)Cg.glo_ni * Cg.glo_nj)) + 1;
@@ -231,10 +233,11 @@ __global__ void k_coarsen(const double *f, double *c, const int *levf, Grid2 F, 
         sa += v;
         if (levf[q2] >= kl) { sw += v; ++nw; }
       }
-    const double m = nw ? sw / nw : sa / (factor * factor);
+    double m = nw ? sw / nw : sa / (factor * factor);
     const int i = I + 2;
-    const long long q = (long long)(i - 1) + (long long)Cg.ni * (J + 1) + Cg.n2 * (k - 1);
-    put_twin(c, Cg, i, q, m);
+    const long long q2c = (long long)(i - 1) + (long long)Cg.ni * (J + 1);
+    if (levc && levc[q2c] < kl) m = 0.0;
+    put_twin(c, Cg, i, q2c + Cg.n2 * (k - 1), m);
   }
 }
 struct CnnStatsDev {
@@ -266,11 +269,11 @@ __global__ void k_cnn_target(const __grid_constant__ Dev Pp, const __grid_consta
     const int I = (int)(p % Pp.glo_ni), J = (int)((p / Pp.glo_ni) % Pp.glo_nj), k = (int)(p / ((long long)Pp.glo_ni * Pp.glo_nj)) + 1;
     const long long q2 = (long long)(I + 1) + (long long)Pp.ni * (J + 1), q = q2 + Pp.n2 * (k - 1);
     const float mu = Pp.lev_u[q2] >= k ? 1.f : 0.f, mt = Pp.lev_t[q2] >= k ? 1.f : 0.f;
-    if (target) {
-      target[p * 4 + 0] = mu * (float)((Pt.uc[q] - Pp.uc[q]) * rdt / st.out_std[0]);
-      target[p * 4 + 1] = mu * (float)((Pt.vc[q] - Pp.vc[q]) * rdt / st.out_std[1]);
-      target[p * 4 + 2] = mt * (float)((Pt.tc[q] - Pp.tc[q]) * rdt / st.out_std[2]);
-      target[p * 4 + 3] = mt * (float)((Pt.sc[q] - Pp.sc[q]) * rdt / st.out_std[3]);
+    if (target) {  // an output with scale 0 carries no signal: target 0
+      const double d[4] = {Pt.uc[q] - Pp.uc[q], Pt.vc[q] - Pp.vc[q], Pt.tc[q] - Pp.tc[q], Pt.sc[q] - Pp.sc[q]};
+      const float m[4] = {mu, mu, mt, mt};
+      for (int c = 0; c < 4; ++c)
+        target[p * 4 + c] = st.out_std[c] > 0.f ? m[c] * (float)(d[c] * rdt / st.out_std[c]) : 0.f;
     }
     if (mask) {
       mask[p * 4 + 0] = mu;
@@ -1332,21 +1335,23 @@ int pcom_gpu_coarsen(pcom_handle *f, pcom_handle *c, int32_t factor) {
   const Grid2 F = grid2(f), Cg = grid2(c);
   Dev &A = f->D, &B = c->D;
   const int nk = c->nk;
-  auto run = [&](const double *src, double *dst, const int *lev, int nlev, int plane) {
-    k_coarsen<<<592, 256, 0, c->stream>>>(src, dst, lev, F, Cg, nlev, factor, plane);
+  auto run = [&](const double *src, double *dst, const int *lev, const int *levc, int nlev, int plane) {
+    k_coarsen<<<592, 256, 0, c->stream>>>(src, dst, lev, levc, F, Cg, nlev, factor, plane);
   };
-  run(A.tc, B.tc, A.lev_t, nk, 1);
-  run(A.sc, B.sc, A.lev_t, nk, 1);
-  if (B.tp != B.tc) { run(A.tp, B.tp, A.lev_t, nk, 1); run(A.sp, B.sp, A.lev_t, nk, 1); }
-  const double *fu[] = {A.uc, A.vc, A.up, A.vp, A.auc, A.aup, A.aupp, A.avc, A.avp, A.avpp, A.am};
-  double *cu[] = {B.uc, B.vc, B.up, B.vp, B.auc, B.aup, B.aupp, B.avc, B.avp, B.avpp, B.am};
-  for (int q = 0; q < 11; ++q) run(fu[q], cu[q], A.lev_u, nk, 1);
+  run(A.tc, B.tc, A.lev_t, nullptr, nk, 1);
+  run(A.sc, B.sc, A.lev_t, nullptr, nk, 1);
+  if (B.tp != B.tc) { run(A.tp, B.tp, A.lev_t, nullptr, nk, 1); run(A.sp, B.sp, A.lev_t, nullptr, nk, 1); }
+  // velocities and their tendencies vanish at the coarse grid's land U points
+  const double *fu[] = {A.uc, A.vc, A.up, A.vp, A.auc, A.aup, A.aupp, A.avc, A.avp, A.avpp};
+  double *cu[] = {B.uc, B.vc, B.up, B.vp, B.auc, B.aup, B.aupp, B.avc, B.avp, B.avpp};
+  for (int q = 0; q < 10; ++q) run(fu[q], cu[q], A.lev_u, B.lev_u, nk, 1);
+  run(A.am, B.am, A.lev_u, nullptr, nk, 1);
   const double *ft[] = {A.chc, A.chp, A.mch, A.mch2};
   double *ct[] = {B.chc, B.chp, B.mch, B.mch2};
-  for (int q = 0; q < 4; ++q) run(ft[q], ct[q], A.lev_t, 1, 0);
+  for (int q = 0; q < 4; ++q) run(ft[q], ct[q], A.lev_t, nullptr, 1, 0);
   const double *fb[] = {A.ubc, A.vbc, A.ubp, A.vbp};
   double *cb[] = {B.ubc, B.vbc, B.ubp, B.vbp};
-  for (int q = 0; q < 4; ++q) run(fb[q], cb[q], A.lev_u, 1, 0);
+  for (int q = 0; q < 4; ++q) run(fb[q], cb[q], A.lev_u, B.lev_u, 1, 0);
   CK(cudaGetLastError());
   c->launches += 21;
   return sync_check(c);

@@ -34,6 +34,10 @@ def test_coarsen_is_block_mean_over_wet_cells():
         num, den = (v * w).sum(axis=(1, 3)), w.sum(axis=(1, 3))
         ref = np.where(den > 0, num / np.maximum(den, 1), v.mean(axis=(1, 3)))
         assert np.abs(got[k] - ref).max() <= 1e-12 * np.abs(ref).max()
+    # velocities vanish at the coarse grid's land U points
+    k = np.arange(1, nk + 1)[:, None, None]
+    land_u = (c.static()["lev_u"][None] < k)[:, 1:-1, 1:-1]
+    assert np.all(c.field("uc")[:, 1:-1, 1:-1][land_u] == 0.0)
     # halo twins of the periodic coarse grid
     full = c.field("tc")
     assert np.array_equal(full[:, :, 0], full[:, :, -2]) and np.array_equal(full[:, :, -1], full[:, :, 1])
