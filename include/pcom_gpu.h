@@ -42,8 +42,10 @@ extern "C" {
  * diffusion, upwelling and Smagorinsky stencils compute in FP32; alpha and
  * adp are stored as anomalies from a reference profile (fixed from the level
  * means of the first T/S given to pcom_gpu_set_state); the barotropic
- * subcycle and its ch/mch/mch2 accumulation, the pressure-gradient and AB3
- * updates, the tracer update and the global sums stay FP64.  The ABI keeps
+ * subcycle computes velocities, fluxes and divergence in FP32 while the
+ * bottom pressure ch, its gradients and its ch/mch/mch2 accumulation stay
+ * FP64, as do the baroclinic pressure-gradient and AB3 updates, the tracer
+ * update and the global sums.  The ABI keeps
  * FP64 host arrays: the library converts on upload and download.  No
  * counterpart in the reference. */
 #define PCOM_PREC_MIXED 0x1

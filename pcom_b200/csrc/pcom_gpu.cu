@@ -569,7 +569,10 @@ int do_trop(pcom_handle *h) {
   cudaError_t e;
   if (h->trop_resident) {
     // the kernel's barrier counter is monotone: pass the arrivals so far
-    e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
+    if (h->mixed && trop_mixed_max_blocks(h->trop_tx, h->trop_ty) >= h->trop_blocks)
+      e = launch_trop_mixed(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
+    else
+      e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
   } else if (h->trop_multi) {
     k_copy_dev<<<1, 256, 0, h->stream>>>(h->D, h->d_dev1);

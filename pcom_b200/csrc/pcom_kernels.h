@@ -46,6 +46,9 @@ int trop_res_max_blocks(int TX, int TY);
 size_t trop_fast_smem_bytes(int TX, int TY);
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
 int trop_fast_max_blocks(int TX, int TY);
+// mixed path: the resident kernel with FP32 arithmetic outside the bottom pressure
+cudaError_t launch_trop_mixed(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
+int trop_mixed_max_blocks(int TX, int TY);
 
 // batched barotropic subcycle: one persistent launch over the tiles of all members
 struct TileRef {
