@@ -678,7 +678,9 @@ __device__ void ts_convect(const DevT<R> &P, long long q2, int nlev, Col c) {
 }
 
 template <typename R, bool BATCH>
-__global__ void __launch_bounds__(512) k_ts(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
+// (FP32 storage: registers for two CTAs per SM)
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) k_ts(const __grid_constant__ DevT<R> P0,
+                                                                    const DevT<R> *__restrict__ Ps) {
   const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
   constexpr bool MIXED = std::is_same<R, float>::value;
   (void)MIXED;
