@@ -171,6 +171,13 @@ int pcom_gpu_int_bnd(pcom_handle *h, int32_t m1, int32_t m2, double f);
  * 3 generic (non-separable metrics).  All give the same results; the choice
  * is for tuning and tests.  No counterpart in the reference. */
 int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which);
+/* Concurrent phases in pcom_gpu_step (on by default): int_readyc's 2-D prep
+ * and upwelling run beside den_alpha and int_pgra, and smag beside int_ssh
+ * and int_ts, on a second stream of the handle forked from and joined back
+ * to the handle's stream by events within each step.  Results are the same
+ * either way; 0 issues every launch on the handle's stream in phase order.
+ * pcom_gpu_phase always runs serially.  No counterpart in the reference. */
+int pcom_gpu_set_overlap(pcom_handle *h, int32_t enable);
 /* Global sums over the wet T cells of the interior: out3[0] = volume (m^3),
  * out3[1] = sum of T dV (K m^3), out3[2] = sum of S dV (psu m^3), with
  * dV = a^2 rh1 dx1x dx1y dz(k); FP64, in a fixed reduction order.  No

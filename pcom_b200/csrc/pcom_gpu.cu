@@ -361,6 +361,11 @@ struct pcom_handle {
   unsigned long long *d_cnt1 = nullptr;
   double *frc_months = nullptr;  // taux, tauy, t, s, pa: [5][12][nj][ni]
   unsigned long long trop_epoch = 0;  // barrier arrivals of the barotropic kernel so far
+  // second stream of the full step: phases that share no array with the
+  // main stream's concurrent phases run on it, forked and joined by events
+  bool overlap = true;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork[2] = {}, ev_join[2] = {};
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
   long long launches = 0;
@@ -384,18 +389,19 @@ namespace {
 struct Prof {
   pcom_handle *h;
   const char *name;
+  cudaStream_t st;
   cudaEvent_t a = nullptr, b = nullptr;
-  Prof(pcom_handle *h_, const char *n) : h(h_), name(n) {
+  Prof(pcom_handle *h_, const char *n, cudaStream_t s = nullptr) : h(h_), name(n), st(s ? s : h_->stream) {
     h->launches++;
     if (h->prof) {
       cudaEventCreate(&a);
       cudaEventCreate(&b);
-      cudaEventRecord(a, h->stream);
+      cudaEventRecord(a, st);
     }
   }
   ~Prof() {
     if (h->prof) {
-      cudaEventRecord(b, h->stream);
+      cudaEventRecord(b, st);
       ProfEntry &e = h->prof_tab[name];
       e.launches++;
       e.pending.emplace_back(a, b);
@@ -405,6 +411,7 @@ struct Prof {
 
 int sync_check(pcom_handle *h) {
   CK(cudaStreamSynchronize(h->stream));
+  if (h->side) CK(cudaStreamSynchronize(h->side));
   CK(cudaGetLastError());
   int err[2] = {0, 0};
   CK(cudaMemcpy(err, h->D.err, sizeof err, cudaMemcpyDeviceToHost));
@@ -526,15 +533,20 @@ int do_pgra(pcom_handle *h) {
   ON_DEV(launch_pgra2d(X, h->stream));
   return PCOM_OK;
 }
-int do_readyc(pcom_handle *h, int64_t iter) {
+// int_readyc's 2-D prep and upwelling (read bnd_pa, chc, chp, uc, vc, wm;
+// write pax, pay, sch_r, sch_w, rsch, rsch2, rchc, wm)
+int do_readyc_2d(pcom_handle *h, cudaStream_t s) {
   {
-    Prof p(h, "readyc_2d");
-    ON_DEV(launch_uv2d(X, 0, h->stream));
+    Prof p(h, "readyc_2d", s);
+    ON_DEV(launch_uv2d(X, 0, s));
   }
   {
-    Prof p(h, "upwelling");
-    ON_DEV(launch_upwelling(X, 0, h->stream));
+    Prof p(h, "upwelling", s);
+    ON_DEV(launch_upwelling(X, 0, s));
   }
+  return PCOM_OK;
+}
+int do_readyc_3d(pcom_handle *h, int64_t iter) {
   // AB3 history: aupp <- aup <- auc (mod_int.f90:115-118) by rotation
   int old_pp = h->ipp;
   h->ipp = h->ip;
@@ -587,7 +599,7 @@ int do_trop(pcom_handle *h) {
   h->n_ch++;
   return PCOM_OK;
 }
-int do_clin(pcom_handle *h) {
+int do_clin_uv(pcom_handle *h) {
   {
     Prof p(h, "clin_2d");
     ON_DEV(launch_uv2d(X, 2, h->stream));
@@ -596,11 +608,13 @@ int do_clin(pcom_handle *h) {
     Prof p(h, "int_clin");
     ON_DEV(launch_clin(X, h->stream));
   }
-  {
-    Prof p(h, "smag");
-    ON_DEV(launch_smag(X, h->stream));
-  }
   h->n_uv++;
+  return PCOM_OK;
+}
+// Smagorinsky viscosity (reads uu, vv, dxs, tn3; writes am, am1)
+int do_smag(pcom_handle *h, cudaStream_t s) {
+  Prof p(h, "smag", s);
+  ON_DEV(launch_smag(X, s));
   return PCOM_OK;
 }
 int do_ssh(pcom_handle *h) {
@@ -636,9 +650,15 @@ int run_phase(pcom_handle *h, int phase, int64_t iter) {
   switch (phase) {
   case 0: return do_den_alpha(h);
   case 1: return do_pgra(h);
-  case 2: return do_readyc(h, iter);
+  case 2: {
+    int rc = do_readyc_2d(h, h->stream);
+    return rc ? rc : do_readyc_3d(h, iter);
+  }
   case 3: return do_trop(h);
-  case 4: return do_clin(h);
+  case 4: {
+    int rc = do_clin_uv(h);
+    return rc ? rc : do_smag(h, h->stream);
+  }
   case 5: return do_ssh(h);
   case 6: return do_ts(h);
   default: return fail(PCOM_ERR_ARG, "unknown phase %d", phase);
@@ -649,10 +669,41 @@ int enqueue_step(pcom_handle *h, int64_t iter) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   if (!h->static_ok) return fail(PCOM_ERR_STATE, "step before pcom_gpu_upload_static");
   if (iter < 1) return fail(PCOM_ERR_ARG, "tctr_i must be >= 1");
-  for (int ph = 0; ph <= 6; ++ph) {
-    int rc = run_phase(h, ph, iter);
-    if (rc) return rc;
+  if (!h->overlap) {
+    for (int ph = 0; ph <= 6; ++ph) {
+      int rc = run_phase(h, ph, iter);
+      if (rc) return rc;
+    }
+    CK(cudaGetLastError());
+    return PCOM_OK;
   }
+  // The same launches in the same per-stream order, with two pairs of
+  // phases that touch no common array run concurrently on the side stream:
+  //  - int_readyc's 2-D prep and upwelling beside den_alpha/int_tobot
+  //    (read tc, sc, chc, alpha; write alpha, adp) and int_pgra (reads
+  //    adp, alpha; writes bphi, bgraphi); joined before int_readyc's 3-D
+  //    part, which reads both sides' results;
+  //  - smag (reads uu, vv; writes am, used by the next step's int_readyc
+  //    and int_trop only) beside int_ssh and int_ts; joined at the end of
+  //    the step.
+  int rc;
+  CK(cudaEventRecord(h->ev_fork[0], h->stream));
+  CK(cudaStreamWaitEvent(h->side, h->ev_fork[0], 0));
+  if ((rc = do_readyc_2d(h, h->side))) return rc;
+  CK(cudaEventRecord(h->ev_join[0], h->side));
+  if ((rc = do_den_alpha(h))) return rc;
+  if ((rc = do_pgra(h))) return rc;
+  CK(cudaStreamWaitEvent(h->stream, h->ev_join[0], 0));
+  if ((rc = do_readyc_3d(h, iter))) return rc;
+  if ((rc = do_trop(h))) return rc;
+  if ((rc = do_clin_uv(h))) return rc;
+  CK(cudaEventRecord(h->ev_fork[1], h->stream));
+  CK(cudaStreamWaitEvent(h->side, h->ev_fork[1], 0));
+  if ((rc = do_smag(h, h->side))) return rc;
+  CK(cudaEventRecord(h->ev_join[1], h->side));
+  if ((rc = do_ssh(h))) return rc;
+  if ((rc = do_ts(h))) return rc;
+  CK(cudaStreamWaitEvent(h->stream, h->ev_join[1], 0));
   CK(cudaGetLastError());
   return PCOM_OK;
 }
@@ -898,6 +949,14 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete h; return fail(PCOM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
   h->own_stream = true;
+  // the side stream and fork/join events of the overlapped step (created
+  // here, not in the step, which may be enqueued into a graph capture)
+  e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+    e = cudaEventCreateWithFlags(&h->ev_fork[q], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join[q], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) { pcom_gpu_destroy(h); return fail(PCOM_ERR_CUDA, "side stream: %s", cudaGetErrorString(e)); }
   Dev &D = h->D;
   D.ni = d.ni; D.nj = d.nj; D.nk = d.nk; D.nkp = d.nk + 1; D.nim = d.ni - 1; D.njm = d.nj - 1;
   D.glo_ni = d.glo_ni; D.glo_nj = d.glo_nj;
@@ -1003,6 +1062,14 @@ int pcom_gpu_destroy(pcom_handle *h) {
   cudaStreamSynchronize(h->stream);
   for (auto &kv : h->prof_tab)
     for (auto &pe : kv.second.pending) { cudaEventDestroy(pe.first); cudaEventDestroy(pe.second); }
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaStreamDestroy(h->side);
+  }
+  for (int q = 0; q < 2; ++q) {
+    if (h->ev_fork[q]) cudaEventDestroy(h->ev_fork[q]);
+    if (h->ev_join[q]) cudaEventDestroy(h->ev_join[q]);
+  }
   for (void *p : h->allocs) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1423,6 +1490,13 @@ int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which) {
   CK(cudaStreamSynchronize(h->stream));
   h->trop_force = which;
   h->trop_blocks = 0;  // re-pick at the next step
+  return PCOM_OK;
+}
+
+int pcom_gpu_set_overlap(pcom_handle *h, int32_t enable) {
+  if (!h) return fail(PCOM_ERR_ARG, "null handle");
+  CK(cudaStreamSynchronize(h->stream));
+  h->overlap = enable != 0;
   return PCOM_OK;
 }
 

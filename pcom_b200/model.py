@@ -162,6 +162,11 @@ class Model:
         L.check(self.lib.pcom_gpu_set_state(self.handle, C.byref(st)), "set_state")
 
     # ------------------------------------------------------------- streams
+    def set_overlap(self, enable: bool):
+        """Concurrent phases in the full step (default on); results are the
+        same either way."""
+        L.check(self.lib.pcom_gpu_set_overlap(self.handle, int(bool(enable))), "set_overlap")
+
     def set_stream(self, stream_ptr: int):
         L.check(self.lib.pcom_gpu_set_stream(self.handle, C.c_void_p(stream_ptr)), "set_stream")
 

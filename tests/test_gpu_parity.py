@@ -132,6 +132,28 @@ def test_barotropic_kernel_forms(oracle_lib, which):
     m.close()
 
 
+@pytest.mark.parametrize("name,mixed", [("global1", False), ("box", False), ("global1", True)])
+def test_overlapped_step_equals_serial(name, mixed):
+    """The full step with its concurrent phases on a second stream (the
+    default) ends bit-equal to the same launches issued serially in phase
+    order, over the AB3 start-up and with per-kernel events on and off."""
+    from pcom_b200 import _lib as L
+
+    c = make_case(name)
+    ms = [Model(c, flags=L.PCOM_PREC_MIXED if mixed else L.PCOM_PREC_FP64) for _ in range(2)]
+    ms[1].set_overlap(False)
+    ms[0].profile(True)
+    for m in ms:
+        m.run(7)
+    lev_t = ms[0].static()["lev_t"]
+    for f in STATE_FIELDS + ["acr"]:
+        mask = acr_mask(lev_t, c["nk"]) if f == "acr" else None
+        r = compare(ms[0].field(f), ms[1].field(f), mask)
+        assert r["unequal"] == 0, f"{name}: {f} differs at {r['unequal']} points"
+    for m in ms:
+        m.close()
+
+
 def test_device_int_bnd_matches_host():
     """The daily forcing interpolated on the device (pcom_gpu_int_bnd, used
     by the time loop) equals the host int_bnd (mod_int.f90:649-691) bitwise."""
