@@ -81,6 +81,26 @@ def test_mixed_state_round_trip():
     mm.close()
 
 
+def test_mixed_over_30_days():
+    """30 model days (720 steps, daily forcing and den_prho) of the 128x64x20
+    box: the mixed path stays within its bounds (measured on B200: tc 4.3e-7,
+    uc 3.7e-5, vc 2.5e-5, chc 3.4e-11, ubc 5.7e-6, vbc 2.4e-6, heat sum
+    9.0e-9), while an FP64 run from a temperature perturbed by N(0, 1e-10 K)
+    stays within 1e-8 of the unperturbed one, so the model does not amplify
+    perturbations over this horizon and the difference is the precision's."""
+    from pcom_b200.precision_report import run
+
+    rep = run("box", [720])
+    e = rep["checkpoints"][-1]
+    bounds = {"tc": 2e-6, "sc": 1e-12, "uc": 2e-4, "vc": 2e-4, "chc": 1e-9, "ubc": 1e-4, "vbc": 1e-4}
+    for f, b in bounds.items():
+        r = e["mixed"]["fields"][f]
+        assert r["finite"] and r["rel_rms"] <= b, f"mixed {f} rel RMS {r['rel_rms']:.3e} > {b:.0e}"
+        assert e["control"]["fields"][f]["rel_rms"] <= 1e-8, f
+    assert e["mixed"]["global_sums"]["heat"] <= 1e-7
+    assert e["mixed"]["global_sums"]["volume"] == 0.0
+
+
 @pytest.mark.parametrize("flags", [L.PCOM_PREC_FP64, L.PCOM_PREC_MIXED])
 def test_global_sums(flags):
     c = make_case("tiny_bathy")
