@@ -9,7 +9,9 @@
 // reference's SUM(..., 3), the cumulative upwelling sum, the column integral
 // of the baroclinic velocity) and the data-dependent convective adjustment
 // are done from shared memory by one thread per column, in the reference's
-// sequential order.  Horizontal operators are evaluated point-wise from their
+// sequential order.  int_ts on the FP64 path is the exception: one thread
+// per column marches down the levels (k_ts_col) and a point-parallel kernel
+// forms the accumulations (k_ts_acc).  Horizontal operators are evaluated point-wise from their
 // definitions in mod_op.f90 (halo conventions in pcom_dev.cuh).  Every
 // division by a static metric, a bottom pressure or a per-step 2-D field uses
 // its precomputed correctly rounded reciprocal with dvr (bitwise equal to the
@@ -626,8 +628,8 @@ struct Col {  // one column of T, S and prho in shared memory, stride TB_X
   __device__ double P2(int k) const { return p2[(k - 1) * TB_X]; }
 };
 
-template <typename R>
-__device__ void ts_mix(const DevT<R> &P, long long q2, Col &c, double *rhoa, double *rhob, int na, int nb) {
+template <typename R, typename C>
+__device__ void ts_mix(const DevT<R> &P, long long q2, C &c, double *rhoa, double *rhob, int na, int nb) {
   double st = 0.0, sd = 0.0;
   for (int k = na; k <= nb; ++k) st = st + c.T(k) * P.dpr2[k];
   for (int k = na; k <= nb; ++k) sd = sd + P.dpr2[k];
@@ -642,8 +644,8 @@ __device__ void ts_mix(const DevT<R> &P, long long q2, Col &c, double *rhoa, dou
   if (nb < P.nk) rhob[nb] = c.P1(nb + 1) * c.T(nb) + c.P2(nb + 1) * c.S(nb);
 }
 
-template <typename R>
-__device__ void ts_convect(const DevT<R> &P, long long q2, int nlev, Col c) {
+template <typename R, typename C>
+__device__ void ts_convect(const DevT<R> &P, long long q2, int nlev, C c) {
   double rhoa[PCOM_MAXK + 2], rhob[PCOM_MAXK + 2];
   for (int k = 0; k <= P.nk + 1; ++k) { rhoa[k] = 0.0; rhob[k] = 0.0; }
   for (int k = 2; k <= nlev; ++k) rhoa[k] = c.P1(k) * c.T(k) + c.P2(k) * c.S(k);
@@ -824,6 +826,210 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) k_ts(const __grid
 }
 
 // ----------------------------------------------------------------------------
+// int_ts on the FP64 path in two kernels (the per-point arithmetic of k_ts
+// above, in the same order).
+//
+// k_ts_col: one thread per column marching down the levels.  The column's
+// masks, 2-D fields and metric factors are read once; the vertical
+// neighbours of T, S, tp, sp, wm and kh roll through registers, so a level
+// reads only the horizontal neighbours.  The new T, S of the column go to
+// the output buffers as they are formed; a column whose density test finds
+// an instability (rhob(k) > rhoa(k+1) for some k < lev) is copied to local
+// arrays, adjusted there (convect) and written back.  The output buffers are
+// never a tracer buffer this kernel reads (three-buffer pool).
+//
+// k_ts_acc: point-parallel, the halo twins of the new T, S and the
+// act/acs/acr accumulations (acr through the equation of state).
+constexpr int kColX = 32, kColY = 2;
+
+// one column of T, S and prho copied to local arrays, levels 1..nlev (+1 for prho)
+struct ColL {
+  double *t, *s, *p1, *p2;
+  __device__ double &T(int k) { return t[k - 1]; }
+  __device__ double &S(int k) { return s[k - 1]; }
+  __device__ double P1(int k) const { return p1[k - 1]; }
+  __device__ double P2(int k) const { return p2[k - 1]; }
+};
+
+template <bool BATCH>
+__global__ void __launch_bounds__(kColX * kColY, 8) k_ts_col(const __grid_constant__ DevT<double> P0,
+                                                            const DevT<double> *__restrict__ Ps) {
+  using R = double;
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  const int x = blockIdx.x * kColX + threadIdx.x;
+  const int j = blockIdx.y * kColY + threadIdx.y + 1;
+  if (x >= P.glo_ni || j > P.nj) return;
+  const int i = x + 2;
+  const int nk = P.nk;
+  const long long n2 = P.n2;
+  const long long q2 = I2(P, i, j);
+  const int ni = P.ni;
+  const R g = P.c.g;
+  const R grho = g * P.c.rho0;
+  const bool nrow = j <= P.njm, srow = j >= 2;
+  const long long qw = q2 - 1, qs = q2 - ni, qsw = qs - 1, qe = q2 + 1, qn = q2 + ni;
+  const int lev = P.lev_t[q2];
+  // column constants (k_ts: the per-point prologue)
+  const int lw = P.lev_t[qw], le = P.lev_t[qe], ln = nrow ? P.lev_t[qn] : 0, ls = srow ? P.lev_t[qs] : 0;
+  const R rh4c = RH(4, j), rh4s = srow ? RH(4, j - 1) : 0.0;
+  const R sc_c = ld(P.sch_r, q2), sc_w = ld(P.sch_r, qw);
+  const R sc_s = srow ? ld(P.sch_r, qs) : 0.0, sc_sw = srow ? ld(P.sch_r, qsw) : 0.0;
+  const R r3c = RH(3, j), r3s = srow ? RH(3, j - 1) : 0.0;
+  const R mc = ld(P.mch, q2), me = ld(P.mch, qe), mw = ld(P.mch, qw);
+  const R mn = nrow ? ld(P.mch, qn) : 0.0, ms = srow ? ld(P.mch, qs) : 0.0;
+  const R c1c = 0.5 * (mc + me), c1w = 0.5 * (mw + mc);
+  const R c2c = nrow ? 0.5 * (mc + mn) : 0.0, c2s = srow ? 0.5 * (ms + mc) : 0.0;
+  const R bc = (R)P.bc;
+  const double rmc = ld(P.rmch, q2);
+  // metric factors of the divisions (the DIVX/DIVY/DIVARH operands)
+  const R mx2c = MX(2, i), rmx2c = RMX(2, i), mx2w = MX(2, i - 1), rmx2w = RMX(2, i - 1);
+  const R mx1c = MX(1, i), rmx1c = RMX(1, i);
+  const R my4c = MY(4, j), rmy4c = RMY(4, j), my1c = MY(1, j), rmy1c = RMY(1, j);
+  const R my4s = srow ? MY(4, j - 1) : 1.0, rmy4s = srow ? RMY(4, j - 1) : 1.0;
+  const R arh1 = ARH(1, j), rarh1 = RARH(1, j), arh2 = ARH(2, j), rarh2 = RARH(2, j);
+  // rolling vertical neighbours: x(k-1), x(k)
+  R tc_m = 0, tc_c = ld(P.tc, q2), sc_m = 0, sc_cc = ld(P.sc, q2);
+  R tp_m = 0, tp_c = ld(P.tp, q2), sp_m = 0, sp_c = ld(P.sp, q2);
+  R wm_c = ld(P.wm, q2), kh_c = ld(P.kh, q2);
+  double t_prev = 0.0, s_prev = 0.0;
+  bool unstable = false;
+  for (int k = 1; k <= nk; ++k) {
+    const long long o = n2 * (k - 1), q = q2 + o;
+    const R m_c = (R)(lev >= k), m_w = (R)(lw >= k), m_e = (R)(le >= k);
+    const R m_n = (R)(ln >= k), m_s = (R)(ls >= k);
+    const R m_k1 = (R)(lev >= k + 1), m_km = (R)(lev >= k - 1);
+    // mass-weighted velocity: um1 = uc*sch on U, um2 = vc*sch*rh3
+    const R um1c = ld(P.uc, q) * sc_c, um1w = ld(P.uc, qw + o) * sc_w;
+    const R um1s = srow ? ld(P.uc, qs + o) * sc_s : 0.0, um1sw = srow ? ld(P.uc, qsw + o) * sc_sw : 0.0;
+    const R um2c = ld(P.vc, q) * sc_c * r3c, um2w = ld(P.vc, qw + o) * sc_w * r3c;
+    const R um2s = srow ? ld(P.vc, qs + o) * sc_s * r3s : 0.0;
+    const R um2sw = srow ? ld(P.vc, qsw + o) * sc_sw * r3s : 0.0;
+    const R wa1c = srow ? 0.5 * (um1s + um1c) : 0.0, wa1w = srow ? 0.5 * (um1sw + um1w) : 0.0;
+    const R wa2c = 0.5 * (um2w + um2c), wa2s = srow ? 0.5 * (um2sw + um2s) : 0.0;
+    const R wmk = wm_c, wmk1 = ld(P.wm, q + n2);  // wm has nkp levels
+    const R khk = kh_c, khk1 = (k < nk) ? ld(P.kh, q + n2) : 0.0;
+    auto adv = [&](const R *var, R xc, R xkm, R xk1) -> R {
+      const R xe = ld(var, qe + o), xw = ld(var, qw + o);
+      const R xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
+      const R w1c = dvr(xe - xc, mx2c, rmx2c), w1w = dvr(xc - xw, mx2w, rmx2w);
+      const R wb1 = 0.5 * (wa1w * w1w + wa1c * w1c);
+      R ans = dvr(wb1, arh1, rarh1);
+      const R w2c = nrow ? dvr(xn - xc, my4c, rmy4c) : 0.0;
+      R wb2 = 0.0;
+      if (srow) {
+        const R w2s = dvr(xc - xs, my4s, rmy4s);
+        wb2 = 0.5 * (wa2s * w2s + wa2c * w2c);
+      }
+      ans = ans + dvr(wb2, arh1, rarh1);
+      const R wmp_k = (k >= 2) ? wmk * (xkm - xc) : wmk * 0.0;
+      const R wmp_k1 = (k < nk) ? wmk1 * (xc - xk1) : wmk1 * 0.0;
+      ans = ans + DIVDP((wmp_k + wmp_k1) * 0.5, k);
+      return ans;
+    };
+    auto dif = [&](const R *var, R xc, R xkm, R xk1) -> R {
+      const R xe = ld(var, qe + o), xw = ld(var, qw + o);
+      const R xn = nrow ? ld(var, qn + o) : 0.0, xs = srow ? ld(var, qs + o) : 0.0;
+      const R w1c = dvr(dvr((xe - xc) * m_e * m_c, mx2c, rmx2c), arh2, rarh2);
+      const R w1w = dvr(dvr((xc - xw) * m_c * m_w, mx2w, rmx2w), arh2, rarh2);
+      const R A = dvr(c1c * w1c - c1w * w1w, mx1c, rmx1c);
+      const R w2c = nrow ? DIVA(dvr((xn - xc) * m_n * m_c, my4c, rmy4c)) : 0.0;
+      R B = 0.0;
+      if (srow) {
+        const R w2s = DIVA(dvr((xc - xs) * m_c * m_s, my4s, rmy4s));
+        B = dvr((c2c * w2c) * rh4c - (c2s * w2s) * rh4s, my1c, rmy1c);
+      }
+      R ans = P.c.ah_c * dvr(A + B, arh1, rarh1);
+      R wkp_k = 0.0, wkp_k1 = 0.0;
+      if (k >= 2) {
+        const R pz = dvr((xkm - xc) * m_km * m_c, P.dz1[k], P.rdz1[k]);
+        wkp_k = grho * khk * pz;
+      }
+      if (k < nk) {
+        const R pz = dvr((xc - xk1) * m_c * m_k1, P.dz1[k + 1], P.rdz1[k + 1]);
+        wkp_k1 = grho * khk1 * pz;
+      }
+      ans = ans + DIVDP(wkp_k - wkp_k1, k);
+      return ans;
+    };
+    const R tc_k1 = (k < nk) ? ld(P.tc, q + n2) : 0.0, sc_k1 = (k < nk) ? ld(P.sc, q + n2) : 0.0;
+    const R tp_k1 = (k < nk) ? ld(P.tp, q + n2) : 0.0, sp_k1 = (k < nk) ? ld(P.sp, q + n2) : 0.0;
+    const R at = adv(P.tc, tc_c, tc_m, tc_k1), as = adv(P.sc, sc_cc, sc_m, sc_k1);
+    const R dt_ = dif(P.tp, tp_c, tp_m, tp_k1), ds_ = dif(P.sp, sp_c, sp_m, sp_k1);
+    R p1 = -at, p2 = -as;
+    p1 = p1 + dt_;
+    p2 = p2 + ds_;
+    if (k == 1) {
+      p1 = p1 + DIVDP(P.c.gamma_t * (ld(P.bnd_t, q2) - tc_c) * m_c, 1);
+      p2 = p2 + P.c.gamma_s * (ld(P.bnd_s, q2) - sc_cc) * m_c * mc;
+    }
+    double tn = (double)tp_c + dvr((double)(p1 * bc * m_c), (double)mc, rmc);
+    const double sn = (double)sp_c + dvr((double)(p2 * bc * m_c), (double)mc, rmc);
+    if (m_c > 0 && tn < P.c.tice) tn = P.c.tice;
+    P.tn_[q] = tn;
+    P.sn_[q] = sn;
+    // convect's trigger: rhob(k-1) > rhoa(k) for 1 <= k-1 < lev
+    if (k >= 2 && k <= lev) {
+      const double2 pr = P.prho[q];
+      const double rb = pr.x * t_prev + pr.y * s_prev;
+      const double ra = pr.x * tn + pr.y * sn;
+      if (rb > ra) unstable = true;
+    }
+    t_prev = tn;
+    s_prev = sn;
+    tc_m = tc_c; tc_c = tc_k1; sc_m = sc_cc; sc_cc = sc_k1;
+    tp_m = tp_c; tp_c = tp_k1; sp_m = sp_c; sp_c = sp_k1;
+    wm_c = wmk1; kh_c = khk1;
+  }
+  if (lev > 1 && unstable) {
+    // convect reads prho one level below the adjusted range
+    double t[PCOM_MAXK], s_[PCOM_MAXK], p1[PCOM_MAXK], p2[PCOM_MAXK];
+    const int np = lev < nk ? lev + 1 : nk;
+    for (int k = 1; k <= np; ++k) {
+      const long long q = q2 + n2 * (k - 1);
+      const double2 pr = P.prho[q];
+      p1[k - 1] = pr.x;
+      p2[k - 1] = pr.y;
+      t[k - 1] = P.tn_[q];
+      s_[k - 1] = P.sn_[q];
+    }
+    ts_convect(P, q2, lev, ColL{t, s_, p1, p2});
+    for (int k = 1; k <= lev; ++k) {
+      const long long q = q2 + n2 * (k - 1);
+      P.tn_[q] = t[k - 1];
+      P.sn_[q] = s_[k - 1];
+    }
+  }
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(512, 2) k_ts_acc(const __grid_constant__ DevT<double> P0,
+                                                const DevT<double> *__restrict__ Ps) {
+  const DevT<double> &P = BATCH ? Ps[blockIdx.z] : P0;
+  int i, j;
+  if (!cell(P, i, j, true)) return;
+  const long long q2 = I2(P, i, j);
+  const int lev = P.lev_t[q2];
+  const double chc = ld(P.chc, q2);
+  const int ni = P.ni;
+  const bool twin = i == 2 || i == ni - 1;
+  const long long dq = i == 2 ? (long long)(ni - 2) : -(long long)(ni - 2);
+  for (int k = threadIdx.y + 1; k <= P.nk; k += TB_K) {
+    const long long q = q2 + P.n2 * (k - 1);
+    const double tn = P.tn_[q], sn = P.sn_[q];
+    if (twin) {
+      P.tn_[q + dq] = tn;
+      P.sn_[q + dq] = sn;
+    }
+    st2(P.act, P, i, q, P.act[q] + tn);
+    st2(P.acs, P, i, q, P.acs[q] + sn);
+    if (k <= lev) {
+      const double w = 1.0 / den_rho(P.c, tn, sn, chc * P.pr2[k]);
+      st2(P.acr, P, i, q, P.acr[q] + 1.0 / w);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
 // den_prho (mod_den.f90:120-153)
 template <typename R, bool BATCH>
 __global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
@@ -884,7 +1090,14 @@ void launch_smag(const DevT<R> &P, cudaStream_t s) {
 template <typename R>
 void launch_ssh(const DevT<R> &P, cudaStream_t s) { k_ssh<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
 template <typename R>
-void launch_ts(const DevT<R> &P, cudaStream_t s) { k_ts<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
+void launch_ts(const DevT<R> &P, cudaStream_t s) {
+  if constexpr (std::is_same<R, double>::value) {
+    k_ts_col<false><<<dim3((P.glo_ni + kColX - 1) / kColX, (P.nj + kColY - 1) / kColY), dim3(kColX, kColY), 0, s>>>(P, nullptr);
+    k_ts_acc<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr);
+  } else {
+    k_ts<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr);
+  }
+}
 template <typename R>
 void launch_den_prho(const DevT<R> &P, cudaStream_t s) { k_den_prho<R, false><<<g3(P.ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr); }
 
@@ -916,7 +1129,10 @@ void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cuda
   case BK_CLIN: k_clin<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
   case BK_SMAG: k_smag<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
   case BK_SSH: k_ssh<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
-  case BK_TS: k_ts<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
+  case BK_TS:
+    k_ts_col<true><<<dim3((b.glo_ni + kColX - 1) / kColX, (b.nj + kColY - 1) / kColY, n), dim3(kColX, kColY), 0, s>>>(none, dPs);
+    k_ts_acc<true><<<g3(b.glo_ni, b.nj, n), kBlock3, 0, s>>>(none, dPs);
+    break;
   case BK_DEN_PRHO: k_den_prho<double, true><<<g3(b.ni, b.nj, n), kBlock3, 0, s>>>(none, dPs); break;
   default: break;
   }

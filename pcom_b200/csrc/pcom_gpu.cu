@@ -636,6 +636,7 @@ int do_ts(pcom_handle *h) {
   {
     Prof p(h, "int_ts");
     ON_DEV(launch_ts(X, h->stream));
+    if (!h->mixed) h->launches++;  // FP64: the column kernel and the accumulation kernel
   }
   // tc = tp = the buffer just written (mod_int.f90:496-497)
   int fr = 0;
@@ -1874,7 +1875,7 @@ int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
   if (rc) return rc;
   rc = batch_join_out(b);
   if (rc) return rc;
-  b->launches += 12 + (int64_t)b->groups.size();  // kernels of one batched step
+  b->launches += 13 + (int64_t)b->groups.size();  // kernels of one batched step
   for (pcom_handle *h : b->hs) {
     h->D.ab3_mode = 0;
     h->n_ch++; h->n_uv++; h->n_ssh++; h->n_w++; h->n_ts++;
