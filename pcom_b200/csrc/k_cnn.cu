@@ -246,178 +246,294 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__res
 
 // ----------------------------------------------------------------------------
 // Persistent form of the same convolution.  A tile is 128 consecutive pixels
-// of one image row; its 3 x 130 halo of input pixels is loaded once into
-// shared memory "chunk-planar" (plane c holds channels 8c..8c+7 of every
-// halo pixel, 16 bytes per pixel, pixels contiguous), so that the A operand
-// of tap (dy, dx) is the same planes read from a start address shifted by
-// (dy + 1) * 130 + (dx + 1) pixels: leading byte offset = plane size (K
-// direction), stride byte offset = 128 bytes (8 pixels).  All 9 taps of the
-// weights stay in shared memory for the kernel's lifetime; the next tile's
-// halo loads while the tensor cores work on the current one.
-constexpr int kHaloW = kM + 2;                 // halo columns
-constexpr int kPlane = 3 * kHaloW * 16;        // bytes per 8-channel plane
+// of one image row.  Each CTA walks a contiguous strip of tiles down the rows
+// of one column of tiles, so consecutive tiles share two of their three halo
+// rows: the halo rows live in a ring of 4 slots in shared memory
+// "chunk-planar" (plane c holds channels 8c..8c+7, 16 bytes per pixel, a
+// slot's 130 pixels contiguous), and each tile loads one new row.  The A
+// operand of tap (dy, dx) is the planes of the slot holding row y + dy read
+// from pixel dx + 1: leading byte offset = plane size (K direction), stride
+// byte offset = 128 bytes (8 pixels).  Taps whose row falls outside the
+// image are skipped (their contribution is zero).  All 9 taps of the weights
+// stay in shared memory for the kernel's lifetime.
+//
+// Two accumulators in tensor memory: the MMAs of tile i+1 are issued as soon
+// as those of tile i complete, so the tensor cores work on tile i+1 while the
+// CTA drains tile i's accumulator and loads the row tile i+2 adds.  Warps w
+// and w+4 read lane quarter w%4 of the accumulator, each half of its columns.
+constexpr int kHaloW = kM + 2;               // halo columns
+constexpr int kRing = 4;                     // halo row slots
+constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 bytes)
+constexpr int kRPlane = kRing * kRowB;       // one 8-channel plane of the ring
+constexpr int kHThreads = 256;               // 8 warps: two per TMEM lane quarter
 
 template <int CIN, int NOUT>
-__global__ void __launch_bounds__(kThreads) k_conv_halo(const __nv_bfloat16 *__restrict__ in,
-                                                        const __nv_bfloat16 *__restrict__ w,
-                                                        const float *__restrict__ bias,
-                                                        const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
-                                                        int H, int W, int periodic_x, int mode, int nstore, int *err) {
+__global__ void __launch_bounds__(kHThreads) k_conv_halo(const __nv_bfloat16 *__restrict__ in,
+                                                         const __nv_bfloat16 *__restrict__ w,
+                                                         const float *__restrict__ bias,
+                                                         const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
+                                                         int H, int W, int periodic_x, int mode, int nstore, int *err) {
   constexpr int KC = CIN / 8;
   constexpr int W_BYTES = 9 * NOUT * CIN * 2;
-  constexpr int A_BYTES = KC * kPlane;
+  constexpr int A_BYTES = KC * kRPlane;
   constexpr int ROWB = NOUT * 2 + 16;  // padded BF16 row of the output staging tile
   constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
+  constexpr int NSPLIT = NOUT >= 32 ? 2 : 1;  // warps sharing a lane quarter's columns
+  constexpr int CPW = NOUT / NSPLIT;          // accumulator columns per warp
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[2];  // MMAs of accumulator b done
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  uint8_t *Wsm = smem, *Abuf[2] = {smem + W_BYTES, smem + W_BYTES + A_BYTES};
-  uint8_t *Osm = smem + W_BYTES + 2 * A_BYTES;  // kM rows of ROWB bytes
+  const int quarter = warp & 3, half = warp >> 2;
+  uint8_t *Wsm = smem, *Ring = smem + W_BYTES, *Osm = smem + W_BYTES + A_BYTES;
   const int ntx = (W + kM - 1) / kM;
-  const long long ntiles = (long long)nimg * H * ntx;
+  const long long NR = (long long)nimg * H;  // image rows
+  const long long ntiles = NR * ntx;
+  // this CTA's strip: tiles t0..t1-1, t = tx * NR + (img * H + y)
+  const long long chunk = (ntiles + gridDim.x - 1) / gridDim.x;
+  const long long t0 = (long long)blockIdx.x * chunk;
+  const long long t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
 
-  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), NCOLS);
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), 2 * NCOLS);
   if (tid == 0) {
-    mbar_init(smem_u32(&mbar), 1);
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // weights: tap t, core matrix (n/8, c) at t*NOUT*CIN*2 + ((n/8)*KC + c)*128 + (n%8)*16
-  for (int q = tid; q < 9 * NOUT * KC; q += kThreads) {
+  for (int q = tid; q < 9 * NOUT * KC; q += kHThreads) {
     const int t = q / (NOUT * KC), r = q % (NOUT * KC), n = r / KC, c = r % KC;
     const uint32_t dst = smem_u32(Wsm) + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16);
     cp_async16(dst, w + ((long long)t * NOUT + n) * CIN + c * 8, true);
   }
-  auto load_halo = [&](long long tile, uint8_t *A) {
-    const int tx = (int)(tile % ntx);
-    const long long row = tile / ntx;  // img * H + y
-    const int y = (int)(row % H);
-    const long long img = row / H;
+  // a tile's position: column tile, image row gr = img * H + y, and y
+  struct Pos {
+    int tx, gr, y;
+  };
+  // the tile after `a` in t order (rows first, then column tiles)
+  auto advance = [&](Pos a) {
+    ++a.gr;
+    if (++a.y == H) a.y = 0;
+    if (a.gr == (int)NR) {
+      a.gr = 0;
+      a.y = 0;
+      ++a.tx;
+    }
+    return a;
+  };
+  // ring bookkeeping, identical in every thread: slot s holds image row
+  // tag_row[s] of column tile tag_tx[s]
+  int tag_row[kRing] = {-1, -1, -1, -1};
+  int tag_tx[kRing] = {-1, -1, -1, -1};
+  // row gr (= img * H + y) of column tile tx into slot gr % 4 (cp.async)
+  auto load_row = [&](int tx, int gr) {
+    const int s = gr & 3;
     const int x0 = tx * kM;
-    for (int q = tid; q < 3 * kHaloW * KC; q += kThreads) {
-      const int pix = q / KC, c = q % KC, r = pix / kHaloW, u = pix % kHaloW;
-      const int yy = y + r - 1;
+    for (int q = tid; q < kHaloW * KC; q += kHThreads) {
+      const int u = q / KC, c = q % KC;
       int xx = x0 - 1 + u;
-      bool ok = yy >= 0 && yy < H;
+      bool ok = true;
       if (xx < 0 || xx >= W) {
-        if (periodic_x) xx = ((xx % W) + W) % W;
-        else ok = false;
+        if (periodic_x) {
+          if (xx < 0) xx += W;  // x0 - 1 >= -1
+          else if ((xx -= W) >= W) xx %= W;
+        } else {
+          ok = false;
+        }
       }
-      const long long src = (img * H + yy) * W + xx;
-      const uint32_t dst = smem_u32(A) + (uint32_t)(c * kPlane + pix * 16);
-      cp_async16(dst, ok ? (const void *)(in + src * CIN + c * 8) : (const void *)in, ok);
+      const uint32_t dst = smem_u32(Ring) + (uint32_t)(c * kRPlane + s * kRowB + u * 16);
+      cp_async16(dst, ok ? (const void *)(in + ((long long)gr * W + xx) * CIN + c * 8) : (const void *)in, ok);
+    }
+    tag_row[s] = gr;
+    tag_tx[s] = tx;
+  };
+  // the image rows a tile reads: y - 1, y, y + 1 inside the image
+  auto row_used = [&](const Pos &a, int dy) { return a.y + dy >= 0 && a.y + dy < H; };
+  // whether the rows of tile `a` missing from the ring go to slots that tile
+  // `busy` (whose MMAs may be in flight) does not read
+  auto can_load = [&](const Pos &a, const Pos &busy) {
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (!row_used(a, dy)) continue;
+      const int s = (a.gr + dy) & 3;
+      if (tag_row[s] == a.gr + dy && tag_tx[s] == a.tx) continue;
+      for (int by = -1; by <= 1; ++by)
+        if (row_used(busy, by) && ((busy.gr + by) & 3) == s) return false;
+    }
+    return true;
+  };
+  auto ensure_rows = [&](const Pos &a) {
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (!row_used(a, dy)) continue;
+      const int s = (a.gr + dy) & 3;
+      if (!(tag_row[s] == a.gr + dy && tag_tx[s] == a.tx)) load_row(a.tx, a.gr + dy);
     }
   };
-  long long tile = blockIdx.x;
-  if (tile < ntiles) load_halo(tile, Abuf[0]);
+  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
+  // descriptors with the start address at the ring and at the weights; the
+  // others differ only in the start address field (address >> 4 in the low
+  // 14 bits; shared memory addresses stay below 256 KB, so it never carries)
+  const uint64_t adesc0 = umma_desc(smem_u32(Ring), kRPlane, 128);
+  const uint64_t bdesc0 = umma_desc(smem_u32(Wsm), 128, KC * 128);
+  // the taps of tile `a` inside the image x CIN/16 K-steps into accumulator
+  // `acc` (one thread)
+  auto issue_mma = [&](const Pos &a, uint32_t acc, uint32_t mb) {
+    tc_fence_after();
+    uint32_t accum = 0;
+    #pragma unroll
+    for (int tp = 0; tp < 9; ++tp) {
+      const int dy = tp / 3 - 1, dx = tp % 3 - 1;
+      if (!row_used(a, dy)) continue;
+      const int s = (a.gr + dy) & 3;
+      #pragma unroll
+      for (int j = 0; j < CIN / 16; ++j) {
+        const uint64_t ad = adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kRPlane) >> 4);
+        const uint64_t bd = bdesc0 + (uint64_t)((tp * NOUT * CIN * 2 + j * 256) >> 4);
+        umma_bf16(acc, ad, bd, idesc, accum);
+        accum = 1u;
+      }
+    }
+    umma_commit(mb);
+  };
+  uint32_t ph[2] = {0, 0};
+  bool mpend = false;  // an MMA group issued and not yet waited for
+  int mpend_b = 0;
+  bool fail = false;
+  bool deferred = false;  // the next tile's rows are loaded after the current tile's MMAs
+  long long tile = t0;
+  // positions of tiles tile, tile + 1, tile + 2
+  Pos p0{0, 0, 0};
+  if (t0 < t1) {
+    p0.tx = (int)(t0 / NR);
+    p0.gr = (int)(t0 % NR);
+    p0.y = p0.gr % H;
+  }
+  Pos p1 = advance(p0), p2 = advance(p1);
+  if (tile < t1) ensure_rows(p0);
+  cp_async_wait_all();  // the weights and the first tile's rows
+  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
-    uint8_t *A = Abuf[it & 1];
-    cp_async_wait_all();  // this tile's halo (and, the first time, the weights)
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      #pragma unroll
-      for (int t = 0; t < 9; ++t) {
-        #pragma unroll
-        for (int j = 0; j < CIN / 16; ++j) {
-          const uint32_t a0 = smem_u32(A) + (uint32_t)(((t / 3) * kHaloW + (t % 3)) * 16 + 2 * j * kPlane);
-          const uint64_t ad = umma_desc(a0, kPlane, 128);
-          const uint64_t bd = umma_desc(smem_u32(Wsm) + (uint32_t)(t * NOUT * CIN * 2 + j * 256), 128, KC * 128);
-          umma_bf16(tmem, ad, bd, idesc, (t > 0 || j > 0) ? 1u : 0u);
-        }
-      }
-      umma_commit(smem_u32(&mbar));
+  if (tile < t1) {
+    if (tid == 0) issue_mma(p0, tmem, smem_u32(&mbar[0]));
+    mpend = true;
+    mpend_b = 0;
+    if (tile + 1 < t1) {
+      if (can_load(p1, p0)) ensure_rows(p1);
+      else deferred = true;
     }
-    // the next tile's halo goes to the other buffer (its last readers, the
-    // previous tile's MMAs, have completed)
-    const long long next = tile + gridDim.x;
-    if (next < ntiles) load_halo(next, Abuf[(it + 1) & 1]);
-    if (!mbar_wait(smem_u32(&mbar), phase)) {
-      ok = false;
-      if (tid == 0) atomicExch(err, 1);
-      mbar_wait(smem_u32(&mbar), phase);  // one more bounded wait for the MMAs in flight
+  }
+  for (int it = 0; tile < t1; ++tile, ++it, p0 = p1, p1 = p2, p2 = advance(p2)) {
+    const int b = it & 1;
+    cp_async_wait_all();  // the next tile's rows (issued one tile earlier)
+    fence_async_smem();
+    const bool done = mbar_wait(smem_u32(&mbar[b]), ph[b]);  // this tile's MMAs
+    if (__syncthreads_or(!done)) {
+      fail = true;
       break;
     }
-    phase ^= 1;
+    ph[b] ^= 1;
+    mpend = false;
+    const bool next = tile + 1 < t1;
+    if (next && deferred) {
+      // the ring slots are free now: load, wait and publish the next rows
+      ensure_rows(p1);
+      cp_async_wait_all();
+      fence_async_smem();
+      __syncthreads();
+      deferred = false;
+    }
     tc_fence_after();
-    const int tx = (int)(tile % ntx);
-    const long long row = tile / ntx;
-    const int m = warp * 32 + lane, x0 = tx * kM, x = x0 + m;
+    if (next) {
+      if (tid == 0) issue_mma(p1, tmem + (uint32_t)(1 - b) * NCOLS, smem_u32(&mbar[1 - b]));
+      mpend = true;
+      mpend_b = 1 - b;
+      // rows of tile + 2, into slots tile + 1 does not read
+      if (tile + 2 < t1) {
+        if (can_load(p2, p1)) ensure_rows(p2);
+        else deferred = true;
+      }
+    }
+    const uint32_t acc = tmem + (uint32_t)b * NCOLS;
+    const int tx = p0.tx;
+    const long long row = p0.gr;
+    const int m = quarter * 32 + lane, x0 = tx * kM, x = x0 + m;
     const int nvalid = min(kM, W - x0);
     const long long p = row * W + x;
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_addr = acc + ((uint32_t)(quarter * 32) << 16);
     if (mode == 2) {
       // the tile's ReLU mask rows, coalesced, into the staging tile
       const uint4 *src = reinterpret_cast<const uint4 *>(aux + (row * W + x0) * NOUT);
-      for (int q = tid; q < nvalid * (NOUT / 8); q += kThreads)
+      for (int q = tid; q < nvalid * (NOUT / 8); q += kHThreads)
         *reinterpret_cast<uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16) = src[q];
       __syncthreads();
     }
-    #pragma unroll
-    for (int c0 = 0; c0 < NOUT; c0 += 16) {
-      float v[16];
-      tmem_ld16(lane_addr + c0, v);
-      if (mode == 1) {
-        if (x < W && c0 == 0) {
-          float *o = (float *)out + p * nstore;
-          if (nstore == 4) {
-            *reinterpret_cast<float4 *>(o) =
-                make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
-          } else {
-            for (int q = 0; q < 16 && q < nstore; ++q) o[q] = v[q] + bias[q];
-          }
-        } else if (x < W) {
-          float *o = (float *)out + p * nstore;
-          for (int q = 0; q < 16; ++q)
-            if (c0 + q < nstore) o[c0 + q] = v[q] + bias[c0 + q];
-        }
-      } else {
-        uint4 *srow = reinterpret_cast<uint4 *>(Osm + m * ROWB + c0 * 2);
-        uint32_t pk[8];
-        if (mode == 0) {
-          #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v[2 * q] + bias[c0 + 2 * q], 0.f),
-                                                            fmaxf(v[2 * q + 1] + bias[c0 + 2 * q + 1], 0.f));
-            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+    if (half < NSPLIT) {
+      #pragma unroll
+      for (int c0 = half * CPW; c0 < (half + 1) * CPW; c0 += 16) {
+        float v[16];
+        tmem_ld16(lane_addr + c0, v);
+        if (mode == 1) {
+          if (x < W && c0 == 0) {
+            float *o = (float *)out + p * nstore;
+            if (nstore == 4) {
+              *reinterpret_cast<float4 *>(o) =
+                  make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
+            } else {
+              for (int q = 0; q < 16 && q < nstore; ++q) o[q] = v[q] + bias[q];
+            }
+          } else if (x < W) {
+            float *o = (float *)out + p * nstore;
+            for (int q = 0; q < 16; ++q)
+              if (c0 + q < nstore) o[c0 + q] = v[q] + bias[c0 + q];
           }
         } else {
-          const uint4 a0 = srow[0], a1 = srow[1];
-          const uint32_t aw[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-          #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw[q]);
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(__low2float(a2) > 0.f ? v[2 * q] : 0.f,
-                                                            __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f);
-            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+          uint4 *srow = reinterpret_cast<uint4 *>(Osm + m * ROWB + c0 * 2);
+          uint32_t pk[8];
+          if (mode == 0) {
+            #pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v[2 * q] + bias[c0 + 2 * q], 0.f),
+                                                              fmaxf(v[2 * q + 1] + bias[c0 + 2 * q + 1], 0.f));
+              pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+            }
+          } else {
+            const uint4 a0 = srow[0], a1 = srow[1];
+            const uint32_t aw[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            #pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw[q]);
+              const __nv_bfloat162 b2 = __floats2bfloat162_rn(__low2float(a2) > 0.f ? v[2 * q] : 0.f,
+                                                              __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f);
+              pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+            }
           }
+          srow[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          srow[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         }
-        srow[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-        srow[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
       }
     }
     if (mode != 1) {
       __syncthreads();
       // the tile's output rows are contiguous in global memory
       uint4 *dst = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (row * W + x0) * NOUT);
-      for (int q = tid; q < nvalid * (NOUT / 8); q += kThreads)
+      for (int q = tid; q < nvalid * (NOUT / 8); q += kHThreads)
         dst[q] = *reinterpret_cast<const uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16);
     }
     tc_fence_before();
-    __syncthreads();  // accumulator and staging tile read before the next tile
+    __syncthreads();  // accumulator b and the staging tile read before they are reused
+  }
+  if (fail) {
+    // a wait gave up: record it, then wait once more (bounded) for the MMAs
+    // still in flight into this CTA's tensor memory
+    if (tid == 0) atomicExch(err, 1);
+    if (mpend) mbar_wait(smem_u32(&mbar[mpend_b]), ph[mpend_b]);
   }
   cp_async_wait_all();
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+  if (warp == 0) tmem_dealloc(tmem, 2 * NCOLS);
 }
 
 // ----------------------------------------------------------------------------
@@ -537,7 +653,7 @@ size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 
 
 template <int CIN, int NOUT>
 size_t halo_smem() {
-  return smem_floor<NOUT>((size_t)9 * NOUT * CIN * 2 + 2 * (size_t)(CIN / 8) * kPlane + (size_t)kM * (NOUT * 2 + 16));
+  return smem_floor<NOUT>((size_t)9 * NOUT * CIN * 2 + (size_t)(CIN / 8) * kRPlane + (size_t)kM * (NOUT * 2 + 16));
 }
 
 template <int CIN, int NOUT>
@@ -553,12 +669,12 @@ cudaError_t conv_halo_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, co
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_halo<CIN, NOUT>, kThreads, sm);
-  const int tmem_cap = 512 / (NOUT < 32 ? 32 : NOUT);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_halo<CIN, NOUT>, kHThreads, sm);
+  const int tmem_cap = 512 / (2 * (NOUT < 32 ? 32 : NOUT));  // two accumulators per CTA
   per = per < 1 ? 1 : (per > tmem_cap ? tmem_cap : per);
   const long long grid = ntiles < (long long)nsm * per ? ntiles : (long long)nsm * per;
-  k_conv_halo<CIN, NOUT><<<(unsigned)grid, kThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
-                                                              nstore, err);
+  k_conv_halo<CIN, NOUT><<<(unsigned)grid, kHThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
+                                                               nstore, err);
   return cudaGetLastError();
 }
 
