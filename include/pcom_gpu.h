@@ -129,6 +129,20 @@ int pcom_gpu_set_state(pcom_handle *h, const pcom_state *s);
 int pcom_gpu_get_state(pcom_handle *h, pcom_state *s);
 /* bnd%* after int_bnd or the 6-hourly file reads (main.f90:164-201). */
 int pcom_gpu_set_forcing(pcom_handle *h, const pcom_forcing *f);
+/* Asynchronous host transfers (no counterpart in the reference), for a
+ * driver that overlaps its I/O with the steps:
+ * pcom_gpu_set_forcing_async stages taux, tauy, t, s and pa (all five
+ * required; fw is not used by the step) in a second set of device forcing
+ * fields on the handle's upload stream and returns; the next step (or phase,
+ * pcom_gpu_set_forcing, pcom_gpu_int_bnd) switches to the staged set after
+ * the upload.  pcom_gpu_get_state_async snapshots the requested fields on
+ * the handle's stream after the work enqueued so far and copies the
+ * snapshots to the host buffers on the download stream, overlapping the
+ * next steps.  Host buffers must stay valid and untouched until pcom_gpu_sync
+ * (or any synchronous call) returns; pinned host memory makes the copies
+ * asynchronous. */
+int pcom_gpu_set_forcing_async(pcom_handle *h, const pcom_forcing *f);
+int pcom_gpu_get_state_async(pcom_handle *h, pcom_state *s);
 /* Accumulators for output() (main.f90:726-760) and their reset. */
 int pcom_gpu_get_accum(pcom_handle *h, pcom_accum *a);
 int pcom_gpu_reset_accum(pcom_handle *h);

@@ -109,6 +109,8 @@ SIGNATURES = {
     "pcom_gpu_global_sums": (C.c_int, [C.c_void_p, dbl_p]),
     "pcom_gpu_set_trop_kernel": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_set_overlap": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcom_gpu_set_forcing_async": (C.c_int, [C.c_void_p, C.POINTER(Forcing)]),
+    "pcom_gpu_get_state_async": (C.c_int, [C.c_void_p, C.POINTER(State)]),
     "pcom_gpu_set_forcing_months": (C.c_int, [C.c_void_p, C.POINTER(Forcing)]),
     "pcom_gpu_int_bnd": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double]),
     "pcom_gpu_coarsen": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),

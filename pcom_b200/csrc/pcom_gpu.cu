@@ -366,6 +366,16 @@ struct pcom_handle {
   bool overlap = true;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork[2] = {}, ev_join[2] = {};
+  // host transfers of the asynchronous calls: forcing on `copy` into a
+  // second set of forcing fields (taux, tauy, bnd_t, bnd_s, bnd_pa) that the
+  // next step switches to; state on `copy_out` from device snapshots taken
+  // on `stream` (two streams, so an upload never queues behind a download
+  // that waits for a step)
+  cudaStream_t copy = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_frc = nullptr, ev_snap = nullptr, ev_d2h = nullptr, ev_frc_free[2] = {};
+  double *frc_buf[2][5] = {};
+  int frc_cur = 0, frc_pending = -1;
+  std::map<std::string, double *> snap;
   bool prof = false;
   std::map<std::string, ProfEntry> prof_tab;
   long long launches = 0;
@@ -412,6 +422,8 @@ struct Prof {
 int sync_check(pcom_handle *h) {
   CK(cudaStreamSynchronize(h->stream));
   if (h->side) CK(cudaStreamSynchronize(h->side));
+  if (h->copy) CK(cudaStreamSynchronize(h->copy));
+  if (h->copy_out) CK(cudaStreamSynchronize(h->copy_out));
   CK(cudaGetLastError());
   int err[2] = {0, 0};
   CK(cudaMemcpy(err, h->D.err, sizeof err, cudaMemcpyDeviceToHost));
@@ -443,6 +455,21 @@ void bind_rotating(pcom_handle *h) {
 // the mixed path's DM shares every FP64 field of D
 void sync_common(pcom_handle *h) {
   if (h->mixed) static_cast<DevCommon &>(h->DM) = static_cast<const DevCommon &>(h->D);
+}
+
+// a forcing staged by pcom_gpu_set_forcing_async becomes the step's forcing:
+// the handle's stream waits for its upload, the set in use so far is free
+// once the work enqueued until now has run, and D points at the staged set
+int apply_staged_forcing(pcom_handle *h) {
+  if (h->frc_pending < 0) return PCOM_OK;
+  CK(cudaStreamWaitEvent(h->stream, h->ev_frc, 0));
+  CK(cudaEventRecord(h->ev_frc_free[h->frc_cur], h->stream));
+  h->frc_cur = h->frc_pending;
+  h->frc_pending = -1;
+  double *const *b = h->frc_buf[h->frc_cur];
+  h->D.taux = b[0]; h->D.tauy = b[1]; h->D.bnd_t = b[2]; h->D.bnd_s = b[3]; h->D.bnd_pa = b[4];
+  sync_common(h);
+  return PCOM_OK;
 }
 
 int pick_trop_config(pcom_handle *h) {
@@ -670,6 +697,7 @@ int enqueue_step(pcom_handle *h, int64_t iter) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   if (!h->static_ok) return fail(PCOM_ERR_STATE, "step before pcom_gpu_upload_static");
   if (iter < 1) return fail(PCOM_ERR_ARG, "tctr_i must be >= 1");
+  if (int rc = apply_staged_forcing(h)) return rc;
   if (!h->overlap) {
     for (int ph = 0; ph <= 6; ++ph) {
       int rc = run_phase(h, ph, iter);
@@ -956,7 +984,12 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
     e = cudaEventCreateWithFlags(&h->ev_fork[q], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join[q], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_frc_free[q], cudaEventDisableTiming);
   }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking);
+  for (cudaEvent_t *ev : {&h->ev_frc, &h->ev_snap, &h->ev_d2h})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   if (e != cudaSuccess) { pcom_gpu_destroy(h); return fail(PCOM_ERR_CUDA, "side stream: %s", cudaGetErrorString(e)); }
   Dev &D = h->D;
   D.ni = d.ni; D.nj = d.nj; D.nk = d.nk; D.nkp = d.nk + 1; D.nim = d.ni - 1; D.njm = d.nj - 1;
@@ -1070,7 +1103,15 @@ int pcom_gpu_destroy(pcom_handle *h) {
   for (int q = 0; q < 2; ++q) {
     if (h->ev_fork[q]) cudaEventDestroy(h->ev_fork[q]);
     if (h->ev_join[q]) cudaEventDestroy(h->ev_join[q]);
+    if (h->ev_frc_free[q]) cudaEventDestroy(h->ev_frc_free[q]);
   }
+  for (cudaStream_t cs : {h->copy, h->copy_out})
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
+  for (cudaEvent_t ev : {h->ev_frc, h->ev_snap, h->ev_d2h})
+    if (ev) cudaEventDestroy(ev);
   for (void *p : h->allocs) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1262,11 +1303,79 @@ int pcom_gpu_get_state(pcom_handle *h, pcom_state *s) {
 int pcom_gpu_set_forcing(pcom_handle *h, const pcom_forcing *f) {
   if (!h || !f) return fail(PCOM_ERR_ARG, "null argument");
   const long long n2 = h->n2;
+  int rc = apply_staged_forcing(h);
+  if (rc) return rc;
   Dev &D = h->D;
-  int rc = 0;
   auto in = [&](const double *dst, const double *src) { if (!rc) rc = copy_in(h, (double *)dst, src, n2); };
   in(D.taux, f->taux); in(D.tauy, f->tauy); in(D.bnd_t, f->t); in(D.bnd_s, f->s); in(D.bnd_pa, f->pa);
   return rc;
+}
+
+int pcom_gpu_set_forcing_async(pcom_handle *h, const pcom_forcing *f) {
+  if (!h || !f) return fail(PCOM_ERR_ARG, "null argument");
+  const double *src[5] = {f->taux, f->tauy, f->t, f->s, f->pa};
+  for (const double *p : src)
+    if (!p) return fail(PCOM_ERR_ARG, "pcom_gpu_set_forcing_async needs taux, tauy, t, s and pa");
+  const long long n2 = h->n2;
+  if (!h->frc_buf[1][0]) {
+    Dev &D = h->D;
+    double *cur[5] = {const_cast<double *>(D.taux), const_cast<double *>(D.tauy), const_cast<double *>(D.bnd_t),
+                      const_cast<double *>(D.bnd_s), const_cast<double *>(D.bnd_pa)};
+    for (int k = 0; k < 5; ++k) {
+      h->frc_buf[0][k] = cur[k];
+      int rc = h->alloc(&h->frc_buf[1][k], (size_t)n2);
+      if (rc) return rc;
+    }
+  }
+  // the set not in use (or the one already staged); wait until the steps
+  // that read it have run
+  const int tgt = h->frc_pending >= 0 ? h->frc_pending : (h->frc_cur ^ 1);
+  CK(cudaStreamWaitEvent(h->copy, h->ev_frc_free[tgt], 0));
+  for (int k = 0; k < 5; ++k)
+    CK(cudaMemcpyAsync(h->frc_buf[tgt][k], src[k], n2 * sizeof(double), cudaMemcpyHostToDevice, h->copy));
+  CK(cudaEventRecord(h->ev_frc, h->copy));
+  h->frc_pending = tgt;
+  return PCOM_OK;
+}
+
+int pcom_gpu_get_state_async(pcom_handle *h, pcom_state *s) {
+  if (!h || !s) return fail(PCOM_ERR_ARG, "null argument");
+  struct Out { double *dst; const char *name; };
+  const Out outs[] = {{s->tc, "tc"}, {s->sc, "sc"}, {s->tp, "tp"}, {s->sp, "sp"}, {s->uc, "uc"}, {s->vc, "vc"},
+                      {s->up, "up"}, {s->vp, "vp"}, {s->auc, "auc"}, {s->aup, "aup"}, {s->aupp, "aupp"},
+                      {s->avc, "avc"}, {s->avp, "avp"}, {s->avpp, "avpp"}, {s->ubc, "ubc"}, {s->vbc, "vbc"},
+                      {s->ubp, "ubp"}, {s->vbp, "vbp"}, {s->chc, "chc"}, {s->chp, "chp"}, {s->mch, "mch"},
+                      {s->mch2, "mch2"}, {s->am, "am"}, {s->prho, "prho"}, {s->alpha, "alpha"}, {s->adp, "adp"},
+                      {s->wm, "wm"}};
+  // the snapshots are rewritten only after the previous call's host copies
+  CK(cudaStreamWaitEvent(h->stream, h->ev_d2h, 0));
+  std::vector<std::pair<double *, std::pair<const double *, long long>>> jobs;
+  for (const Out &o : outs) {
+    if (!o.dst) continue;
+    Named f = lookup(h, o.name);
+    if (!f.p && !f.pf) return fail(PCOM_ERR_ARG, "unknown field '%s'", o.name);
+    double *&buf = h->snap[o.name];
+    if (!buf) {
+      int rc = h->alloc(&buf, (size_t)f.n);
+      if (rc) return rc;
+    }
+    if (f.p) {
+      CK(cudaMemcpyAsync(buf, f.p, f.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+      const Profile pr = profile_of(h->D);
+      k_to_f64<<<592, 256, 0, h->stream>>>(f.pf, buf, f.n, h->n2, f.per, f.kind, pr);
+      CK(cudaGetLastError());
+      h->launches++;
+    }
+    jobs.push_back({o.dst, {buf, f.n}});
+  }
+  CK(cudaEventRecord(h->ev_snap, h->stream));
+  CK(cudaStreamWaitEvent(h->copy_out, h->ev_snap, 0));
+  for (auto &j : jobs)
+    CK(cudaMemcpyAsync(j.first, j.second.first, j.second.second * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->copy_out));
+  CK(cudaEventRecord(h->ev_d2h, h->copy_out));
+  return PCOM_OK;
 }
 
 int pcom_gpu_get_accum(pcom_handle *h, pcom_accum *a) {
@@ -1318,6 +1427,7 @@ int pcom_gpu_step(pcom_handle *h, int64_t tctr_i) {
 int pcom_gpu_phase(pcom_handle *h, int32_t phase, int64_t tctr_i) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   if (!h->static_ok) return fail(PCOM_ERR_STATE, "phase before pcom_gpu_upload_static");
+  if (int rc = apply_staged_forcing(h)) return rc;
   int rc = run_phase(h, phase, tctr_i);
   if (rc) return rc;
   return sync_check(h);
@@ -1478,6 +1588,7 @@ int pcom_gpu_int_bnd(pcom_handle *h, int32_t m1, int32_t m2, double f) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   if (!h->frc_months) return fail(PCOM_ERR_STATE, "pcom_gpu_int_bnd before pcom_gpu_set_forcing_months");
   if (m1 < 1 || m1 > 12 || m2 < 1 || m2 > 12) return fail(PCOM_ERR_ARG, "months must be 1..12");
+  if (int rc = apply_staged_forcing(h)) return rc;
   Dev &D = h->D;
   k_int_bnd<<<256, 256, 0, h->stream>>>(h->frc_months, (double *)D.taux, (double *)D.tauy, (double *)D.bnd_t,
                                         (double *)D.bnd_s, (double *)D.bnd_pa, h->n2, m1, m2, f);
@@ -1828,6 +1939,8 @@ int pcom_gpu_batch_den_prho(pcom_batch *b) {
 int pcom_gpu_batch_step_async(pcom_batch *b, int64_t tctr_i) {
   if (!b) return fail(PCOM_ERR_ARG, "null batch");
   if (tctr_i < 1) return fail(PCOM_ERR_ARG, "tctr_i must be >= 1");
+  for (pcom_handle *h : b->hs)
+    if (int rc = apply_staged_forcing(h)) return rc;
   // AB3 ring rotation of every member (mod_int.f90:115-118), in lock step
   const int key0 = phase_key(b->hs[0]);
   for (pcom_handle *h : b->hs) {
