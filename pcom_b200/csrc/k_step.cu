@@ -9,9 +9,10 @@
 // reference's SUM(..., 3), the cumulative upwelling sum, the column integral
 // of the baroclinic velocity) and the data-dependent convective adjustment
 // are done from shared memory by one thread per column, in the reference's
-// sequential order.  int_ts on the FP64 path is the exception: one thread
-// per column marches down the levels (k_ts_col) and a point-parallel kernel
-// forms the accumulations (k_ts_acc).  Horizontal operators are evaluated point-wise from their
+// sequential order.  int_ts and int_readyc's 3-D part on the FP64 path are
+// the exceptions: one thread per column marches down the levels (k_ts_col,
+// k_readyc_col), and a point-parallel kernel forms int_ts's accumulations
+// (k_ts_acc).  Horizontal operators are evaluated point-wise from their
 // definitions in mod_op.f90 (halo conventions in pcom_dev.cuh).  Every
 // division by a static metric, a bottom pressure or a per-step 2-D field uses
 // its precomputed correctly rounded reciprocal with dvr (bitwise equal to the
@@ -438,6 +439,183 @@ __global__ void __launch_bounds__(512) k_readyc3d(const __grid_constant__ DevT<R
 }
 
 // ----------------------------------------------------------------------------
+// int_readyc's 3-D part on the FP64 path, one thread per column marching
+// down the levels (the per-point arithmetic of k_readyc3d above, in the same
+// order).  The column's 2-D fields and metric factors are read once; u, v
+// at k-1 and k+1, w on U at k+1 (the next level's w at k) and km roll
+// through registers, so a level reads only the horizontal neighbours of u
+// and v, the four wm of the next level, am and km.  The depth integral of
+// the baroclinic tendency accumulates in registers in level order.
+constexpr int kRcX = 32, kRcY = 2;
+
+template <bool BATCH>
+__global__ void __launch_bounds__(kRcX * kRcY, 7) k_readyc_col(const __grid_constant__ DevT<double> P0,
+                                                              const DevT<double> *__restrict__ Ps) {
+  using R = double;
+  const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
+  const int x = blockIdx.x * kRcX + threadIdx.x;
+  const int j = blockIdx.y * kRcY + threadIdx.y + 1;
+  if (x >= P.glo_ni || j > P.nj) return;
+  const int i = x + 2;
+  const int nk = P.nk;
+  const long long n2 = P.n2;
+  const long long q2 = I2(P, i, j);
+  const int ni = P.ni;
+  const R g = P.c.g, a = P.c.a;
+  const R grho = g * P.c.rho0;
+  const bool nrow = j <= P.njm, srow = j >= 2;
+  const long long qe = q2 + 1, qw = q2 - 1, qn = q2 + ni, qs = q2 - ni;
+  const int lu = P.lev_u[q2];
+  // column constants (k_readyc3d: the per-point prologue)
+  const R sch = ld(P.sch_r, q2), rsch = ld(P.rsch, q2);
+  const R rsc_e = ld(P.rsch, qe), rsc_w = ld(P.rsch, qw);
+  const R sch_e = ld(P.sch_r, qe), sch_w = ld(P.sch_r, qw);
+  const R rh3 = RH(3, j), dx3 = MX(3, i), rdx3 = RMX(3, i), dy3 = MY(3, j), rdy3 = RMY(3, j);
+  const R arh3 = ARH(3, j), rarh3 = RARH(3, j);
+  const R sn = nrow ? ld(P.sch_r, qn) : 1.0, rsn = nrow ? ld(P.rsch, qn) : 1.0;
+  const R ss = srow ? ld(P.sch_r, qs) : 1.0, rss = srow ? ld(P.rsch, qs) : 1.0;
+  const R rh3n = nrow ? RH(3, j + 1) : 0.0, rh3s = srow ? RH(3, j - 1) : 0.0;
+  const R cv1 = ld(P.cv1, q2), cv2 = ld(P.cv2, q2);
+  const R dx4 = MX(4, i), dx4e = MX(4, i + 1), rdx4 = RMX(4, i), rdx4e = RMX(4, i + 1);
+  const R arh4 = ARH(4, j), rarh4 = RARH(4, j);
+  const R my2 = MY(2, j), rmy2 = RMY(2, j);
+  const R my2n = nrow ? MY(2, j + 1) : 1.0, rmy2n = nrow ? RMY(2, j + 1) : 1.0;
+  const R c00 = ld(P.chc, q2), c10 = ld(P.chc, qe);
+  const R c01 = nrow ? ld(P.chc, qn) : 0.0, c11 = nrow ? ld(P.chc, qn + 1) : 0.0;
+  const R chN0 = nrow ? 0.5 * (c00 + c01) : 0.0, chN1 = nrow ? 0.5 * (c10 + c11) : 0.0;
+  const R chE0 = 0.5 * (c00 + c10), chE1 = nrow ? 0.5 * (c01 + c11) : 0.0;
+  const R rh2 = RH(2, j), rh2n = nrow ? RH(2, j + 1) : 0.0;
+  const R dxc = a * RH(4, j) * (dx4 + dx4e);
+  const R rdxc = 1.0 / dxc;
+  const R rsch2 = ld(P.rsch2, q2);
+  const R tx_ = ld(P.taux, q2), ty_ = ld(P.tauy, q2);
+  const R pax = ld(P.pax, q2), pay = ld(P.pay, q2);
+  // w on U: ter_{T->U}(wm / chc) at level kk (rows j <= njm)
+  const R rc00 = ld(P.rchc, q2), rc01 = nrow ? ld(P.rchc, qn) : 1.0;
+  const R rc10 = ld(P.rchc, qe), rc11 = nrow ? ld(P.rchc, qn + 1) : 1.0;
+  auto wU = [&](int kk) -> R {
+    if (!nrow) return 0.0;
+    const long long ok_ = n2 * (kk - 1);
+    return (dvr(ld(P.wm, q2 + ok_), c00, rc00) + dvr(ld(P.wm, qn + ok_), c01, rc01) +
+            dvr(ld(P.wm, qe + ok_), c10, rc10) + dvr(ld(P.wm, qn + 1 + ok_), c11, rc11)) *
+           0.25;
+  };
+  const int lev1 = lu;
+  // rolling: u, v at k-1, k; w on U at k; km at k
+  R u_km = 0.0, v_km = 0.0;
+  R u_c = ld(P.uc, q2), v_c = ld(P.vc, q2);
+  R wUk = wU(1);
+  R km_k = ld(P.km, q2);
+  double su = 0.0, sv = 0.0;
+  for (int k = 1; k <= nk; ++k) {
+    const long long o = n2 * (k - 1);
+    const R mu_k = (R)(lu >= k), mu_k1 = (R)(lu >= k + 1), mu_km = (R)(lu >= k - 1);
+    auto U = [&](long long q) { return ld(P.uc, q + o); };
+    auto V = [&](long long q) { return ld(P.vc, q + o); };
+    // velocities at level k (unweighted wu = uc/sch, wv = vc/sch)
+    const R u_e = U(qe), u_w = U(qw);
+    const R v_e = V(qe), v_w = V(qw);
+    const R wu_c = dvr(u_c, sch, rsch), wu_e = dvr(u_e, sch_e, rsc_e), wu_w = dvr(u_w, sch_w, rsc_w);
+    const R wv_c = dvr(v_c, sch, rsch), wv_e = dvr(v_e, sch_e, rsc_e), wv_w = dvr(v_w, sch_w, rsc_w);
+    R u_n = 0, u_s = 0, v_n = 0, v_s = 0, wu_n = 0, wu_s = 0, wv_n = 0, wv_s = 0;
+    if (nrow) {
+      u_n = U(qn); v_n = V(qn);
+      wu_n = dvr(u_n, sn, rsn); wv_n = dvr(v_n, sn, rsn);
+    }
+    if (srow) {
+      u_s = U(qs); v_s = V(qs);
+      wu_s = dvr(u_s, ss, rss); wv_s = dvr(v_s, ss, rss);
+    }
+    // vertical neighbours at (i, j)
+    const R u_k1 = (k < nk) ? ld(P.uc, q2 + o + n2) : 0.0, v_k1 = (k < nk) ? ld(P.vc, q2 + o + n2) : 0.0;
+    // u on N (i, j), (i+1, j); v*cos on E (i, j), (i, j+1)
+    const R uN0 = 0.5 * (wu_w + wu_c), uN1 = 0.5 * (wu_c + wu_e);
+    const R vE0 = srow ? 0.5 * (wv_s * rh3s + wv_c * rh3) : 0.0;
+    const R vE1 = nrow ? 0.5 * (wv_c * rh3 + wv_n * rh3n) : 0.0;
+    const R wUk1 = wU(k + 1);  // wm has nkp levels
+    const R dm1 = dvr(uN1 - uN0, dx3, rdx3);
+    const R dm2 = nrow ? dvr(vE1 - vE0, dy3, rdy3) : 0.0;
+    const R dw = DIVDP(wUk - wUk1, k);
+    const R rdiv = dvr(dm1 + dm2, arh3, rarh3) + dw;
+    // op_adv(var)
+    auto adv = [&](R x_c, R x_e, R x_w, R x_n, R x_s, R x_km, R x_k1) {
+      const R wk1_0 = (0.5 * (x_w + x_c)) * uN0, wk1_1 = (0.5 * (x_c + x_e)) * uN1;
+      const R wk2_0 = srow ? (0.5 * (x_s + x_c)) * vE0 : 0.0;
+      const R wk2_1 = nrow ? (0.5 * (x_c + x_n)) * vE1 : 0.0;
+      const R wa = dvr(wk1_1 - wk1_0, dx3, rdx3);
+      const R wb = nrow ? dvr(wk2_1 - wk2_0, dy3, rdy3) : 0.0;
+      R ans = dvr(wa + wb, arh3, rarh3);
+      const R wkbp_k = (k >= 2) ? ((x_km + x_c) * 0.5 * wUk) * mu_km * mu_k : 0.0;
+      const R wkbp_k1 = (k < nk) ? ((x_c + x_k1) * 0.5 * wUk1) * mu_k * mu_k1 : 0.0;
+      ans = ans + DIVDP(wkbp_k - wkbp_k1, k);
+      ans = ans - 0.5 * x_c * rdiv;
+      return ans * mu_k;
+    };
+    const R auc = adv(u_c, u_e, u_w, u_n, u_s, u_km, u_k1);
+    const R avc = adv(v_c, v_e, v_w, v_n, v_s, v_km, v_k1);
+    // fri_r3d(ans, sch, v, vp, vc, tau)
+    const R am = ld(P.am, q2 + o);
+    const R km_k1 = ld(P.km, q2 + o + n2);  // km has nkp levels
+    auto fri = [&](R vc_, R ve_, R vw_, R vn_, R vs_, R vp_km, R vp_c, R vp_k1, R vce, R vcw, R v_bot_k,
+                   R vc_bot_k, R v_bot_km, R vc_bot_km, R tau) -> R {
+      const R wx0 = dvr(dvr(vc_ - vw_, dx4, rdx4), arh4, rarh4);
+      const R wx1 = dvr(dvr(ve_ - vc_, dx4e, rdx4e), arh4, rarh4);
+      const R wy0 = srow ? DIVA(dvr(vc_ - vs_, my2, rmy2)) : 0.0;
+      const R wy1 = nrow ? DIVA(dvr(vn_ - vc_, my2n, rmy2n)) : 0.0;
+      const R va0 = chN0 * wx0, va1 = chN1 * wx1;
+      const R vb0 = (chE0 * wy0) * rh2, vb1 = (chE1 * wy1) * rh2n;
+      const R A = dvr(va1 - va0, dx3, rdx3);
+      const R B = nrow ? dvr(vb1 - vb0, dy3, rdy3) : 0.0;
+      const R wka = dvr(A + B, arh3, rarh3);
+      R ans = dvr(am, sch, rsch) * wka;
+      ans = ans + am * cv1 * vp_c;
+      const R pxc = dvr(vce - vcw, dxc, rdxc);
+      ans = ans + am * cv2 * sch * pxc;
+      // wkp at kk = k and k+1: surface stress, bottom drag at lev+1, else
+      // the km-scaled pz (mod_op.f90:147-161)
+      auto wkp = [&](int kk, R vp_a, R vp_b, R v_bot, R vc_bot, R kmv) -> R {
+        if (kk == 1) return dvr(g * tau, sch, rsch);
+        if (lev1 > 0 && kk == lev1 + 1) {
+          const R mag = sqrt(v_bot * v_bot + vc_bot * vc_bot);
+          return dvr(v_bot * g * P.c.cdbot * mag, sch, rsch);
+        }
+        if (kk > nk) return 0.0;
+        const R pzv = dvr((vp_a - vp_b) * (R)(lev1 >= kk - 1) * (R)(lev1 >= kk), P.dz1[kk], P.rdz1[kk]);
+        return dvr(grho * kmv * pzv, sch * sch, rsch2);
+      };
+      const R wkp_k = wkp(k, vp_km, vp_c, v_bot_km, vc_bot_km, km_k);
+      const R wkp_k1 = wkp(k + 1, vp_c, vp_k1, v_bot_k, vc_bot_k, km_k1);
+      return ans * mu_k + DIVDP(wkp_k - wkp_k1, k);
+    };
+    // level k-1 values for a bottom drag at kk = k (lev = k-1)
+    R wu_km = 0.0, wv_km = 0.0;
+    if (k > 1 && lev1 == k - 1) { wu_km = dvr(u_km, sch, rsch); wv_km = dvr(v_km, sch, rsch); }
+    // fx = fri(v = uc/sch, vp = uc, vc = -(vc/sch), taux)
+    const R fx = fri(wu_c, wu_e, wu_w, wu_n, wu_s, u_km, u_c, u_k1, -wv_e, -wv_w, wu_c, -wv_c, wu_km, -wv_km, tx_);
+    // fy = fri(v = vc/sch, vp = vc, vc = uc/sch, tauy)
+    const R fy = fri(wv_c, wv_e, wv_w, wv_n, wv_s, v_km, v_c, v_k1, wu_e, wu_w, wv_c, wu_c, wv_km, wu_km, ty_);
+    const long long q = q2 + o;
+    st2(P.auc, P, i, q, auc);
+    st2(P.avc, P, i, q, avc);
+    if (P.ab3_mode == 1) {
+      st2(P.aup, P, i, q, auc); st2(P.aupp, P, i, q, auc);
+      st2(P.avp, P, i, q, avc); st2(P.avpp, P, i, q, avc);
+    }
+    st2(P.fx, P, i, q, fx);
+    st2(P.fy, P, i, q, fy);
+    const R wx = -auc - sch * P.c.a0 * pax + fx;
+    const R wy = -avc - sch * P.c.a0 * pay + fy;
+    su = su + (double)wx * P.dpr2[k] * (double)mu_k;
+    sv = sv + (double)wy * P.dpr2[k] * (double)mu_k;
+    u_km = u_c; u_c = u_k1; v_km = v_c; v_c = v_k1;
+    wUk = wUk1;
+    km_k = km_k1;
+  }
+  st2(P.ut, P, i, q2, dvr(su, ld(P.prh_u, q2), ld(P.rprh_u, q2)));
+  st2(P.vt, P, i, q2, dvr(sv, ld(P.prh_u, q2), ld(P.rprh_u, q2)));
+}
+
+// ----------------------------------------------------------------------------
 // int_clin (mod_int.f90:298-396): baroclinic momentum, barotropic
 // replacement, unweighted velocity and its accumulation.  smag runs after.
 template <typename R, bool BATCH>
@@ -852,7 +1030,7 @@ struct ColL {
 };
 
 template <bool BATCH>
-__global__ void __launch_bounds__(kColX * kColY, 8) k_ts_col(const __grid_constant__ DevT<double> P0,
+__global__ void __launch_bounds__(kColX * kColY, 7) k_ts_col(const __grid_constant__ DevT<double> P0,
                                                             const DevT<double> *__restrict__ Ps) {
   using R = double;
   const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
@@ -1078,7 +1256,12 @@ void launch_upwelling(const DevT<R> &P, int with_acw, cudaStream_t s) {
   k_upwelling<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 3), s>>>(P, nullptr, with_acw);
 }
 template <typename R>
-void launch_readyc3d(const DevT<R> &P, cudaStream_t s) { k_readyc3d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr); }
+void launch_readyc3d(const DevT<R> &P, cudaStream_t s) {
+  if constexpr (std::is_same<R, double>::value)
+    k_readyc_col<false><<<dim3((P.glo_ni + kRcX - 1) / kRcX, (P.nj + kRcY - 1) / kRcY), dim3(kRcX, kRcY), 0, s>>>(P, nullptr);
+  else
+    k_readyc3d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr);
+}
 template <typename R>
 void launch_clin(const DevT<R> &P, cudaStream_t s) {
   k_clin<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2) + 2 * TB_X * sizeof(double), s>>>(P, nullptr);
@@ -1125,7 +1308,9 @@ void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cuda
   case BK_PGRA2D: k_pgra2d<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
   case BK_UV2D: k_uv2d<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs, arg); break;
   case BK_UPWELLING: k_upwelling<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 3), s>>>(none, dPs, arg); break;
-  case BK_READYC3D: k_readyc3d<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2), s>>>(none, dPs); break;
+  case BK_READYC3D:
+    k_readyc_col<true><<<dim3((b.glo_ni + kRcX - 1) / kRcX, (b.nj + kRcY - 1) / kRcY, n), dim3(kRcX, kRcY), 0, s>>>(none, dPs);
+    break;
   case BK_CLIN: k_clin<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
   case BK_SMAG: k_smag<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
   case BK_SSH: k_ssh<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
