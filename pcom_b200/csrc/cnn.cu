@@ -147,7 +147,12 @@ struct pcom_cnn {
     void *q = nullptr;
     cudaError_t e = cudaMalloc(&q, n * sizeof(T));
     if (e != cudaSuccess) return cfail(PCOM_CNN_ERR_CUDA, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
-    cudaMemset(q, 0, n * sizeof(T));
+    // zeroed on the owning stream and finished before the buffer is handed
+    // out: a plain cudaMemset would run on the legacy stream, which
+    // non-blocking streams are not ordered after, and synchronous copies on
+    // the legacy stream are not ordered after the owning stream either
+    cudaMemsetAsync(q, 0, n * sizeof(T), stream);
+    cudaStreamSynchronize(stream);
     allocs.push_back(q);
     *p = (T *)q;
     return PCOM_CNN_OK;
@@ -359,9 +364,9 @@ int pcom_cnn_conv_layer(int32_t cin, int32_t nout, const void *in, const void *w
                         void *out, int64_t npix, int32_t H, int32_t W, int32_t periodic_x, int32_t mode, int32_t nstore,
                         void *stream) {
   int *err = nullptr;
-  CC(cudaMalloc(&err, sizeof(int)));
-  CC(cudaMemset(err, 0, sizeof(int)));
   cudaStream_t s = (cudaStream_t)stream;
+  CC(cudaMalloc(&err, sizeof(int)));
+  CC(cudaMemsetAsync(err, 0, sizeof(int), s));
   cudaError_t e = cnn_conv(cin, nout, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)w, bias,
                            (const __nv_bfloat16 *)aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
   int h = 0;
@@ -376,9 +381,9 @@ int pcom_cnn_conv_layer(int32_t cin, int32_t nout, const void *in, const void *w
 int pcom_cnn_wgrad_layer(int32_t cin, int32_t nout, const void *in, const void *g, float *dw, int64_t npix, int32_t H,
                          int32_t W, int32_t periodic_x, void *stream) {
   int *err = nullptr;
-  CC(cudaMalloc(&err, sizeof(int)));
-  CC(cudaMemset(err, 0, sizeof(int)));
   cudaStream_t s = (cudaStream_t)stream;
+  CC(cudaMalloc(&err, sizeof(int)));
+  CC(cudaMemsetAsync(err, 0, sizeof(int), s));
   cudaError_t e = cnn_wgrad(cin, nout, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)g, dw, npix, H, W, periodic_x,
                             err, s);
   int h = 0;

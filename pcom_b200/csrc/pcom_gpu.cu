@@ -386,7 +386,12 @@ struct pcom_handle {
     void *q = nullptr;
     cudaError_t e = cudaMalloc(&q, n * sizeof(T));
     if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
-    cudaMemset(q, 0, n * sizeof(T));
+    // zeroed on the owning stream and finished before the buffer is handed
+    // out: a plain cudaMemset would run on the legacy stream, which
+    // non-blocking streams are not ordered after, and synchronous copies on
+    // the legacy stream are not ordered after the owning stream either
+    cudaMemsetAsync(q, 0, n * sizeof(T), stream);
+    cudaStreamSynchronize(stream);
     allocs.push_back(q);
     *p = (T *)q;
     return PCOM_OK;
@@ -428,9 +433,10 @@ int sync_check(pcom_handle *h) {
   int err[2] = {0, 0};
   CK(cudaMemcpy(err, h->D.err, sizeof err, cudaMemcpyDeviceToHost));
   if (err[0]) {
-    cudaMemset(h->D.err, 0, sizeof err);
-    cudaMemset(h->D.bar, 0, 2 * sizeof(unsigned));
-    cudaMemset(h->D.tile_flag, 0, sizeof(unsigned long long));
+    cudaMemsetAsync(h->D.err, 0, sizeof err, h->stream);
+    cudaMemsetAsync(h->D.bar, 0, 2 * sizeof(unsigned), h->stream);
+    cudaMemsetAsync(h->D.tile_flag, 0, sizeof(unsigned long long), h->stream);
+    cudaStreamSynchronize(h->stream);
     h->trop_epoch = 0;
     return fail(PCOM_ERR_TIMEOUT, "a device-side grid barrier gave up waiting (bounded spin)");
   }
@@ -1326,6 +1332,8 @@ int pcom_gpu_set_forcing_async(pcom_handle *h, const pcom_forcing *f) {
       int rc = h->alloc(&h->frc_buf[1][k], (size_t)n2);
       if (rc) return rc;
     }
+    // the upload stream writes the new set only after its zero-fill
+    CK(cudaEventRecord(h->ev_frc_free[1], h->stream));
   }
   // the set not in use (or the one already staged); wait until the steps
   // that read it have run
@@ -1865,7 +1873,8 @@ int batch_sync(pcom_batch *b) {
   int err = 0;
   CK(cudaMemcpy(&err, b->err, sizeof err, cudaMemcpyDeviceToHost));
   if (err) {
-    cudaMemset(b->err, 0, sizeof(int));
+    cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
+    cudaStreamSynchronize(b->stream);
     return fail(PCOM_ERR_TIMEOUT, "a device-side grid barrier of the batch gave up waiting (bounded spin)");
   }
   return PCOM_OK;
@@ -1901,7 +1910,7 @@ int pcom_gpu_batch_create(pcom_handle *const *hs, int32_t n, pcom_batch **out) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&b->cnt, sizeof(unsigned long long));
   if (e == cudaSuccess) { b->allocs.push_back(b->cnt); e = cudaMalloc(&b->err, sizeof(int)); }
-  if (e == cudaSuccess) { b->allocs.push_back(b->err); e = cudaMemset(b->err, 0, sizeof(int)); }
+  if (e == cudaSuccess) { b->allocs.push_back(b->err); e = cudaMemsetAsync(b->err, 0, sizeof(int), b->stream); }
   if (e != cudaSuccess) { delete b; return fail(PCOM_ERR_CUDA, "batch scratch: %s", cudaGetErrorString(e)); }
   int rc = batch_tiles(b, 24, 18);
   if (rc) { delete b; return rc; }
