@@ -192,6 +192,13 @@ int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which);
  * either way; 0 issues every launch on the handle's stream in phase order.
  * pcom_gpu_phase always runs serially.  No counterpart in the reference. */
 int pcom_gpu_set_overlap(pcom_handle *h, int32_t enable);
+/* Longest a device-side wait (a grid barrier of the barotropic kernels) may
+ * take before the kernel gives up, returns early and the next synchronising
+ * call reports PCOM_ERR_TIMEOUT (default 2 s; the barriers normally take
+ * microseconds).  The handle stays usable after a timeout: its barrier
+ * counters are reset, the state of the interrupted step is not meaningful.
+ * No counterpart in the reference. */
+int pcom_gpu_set_wait_limit(pcom_handle *h, double seconds);
 /* Global sums over the wet T cells of the interior: out3[0] = volume (m^3),
  * out3[1] = sum of T dV (K m^3), out3[2] = sum of S dV (psu m^3), with
  * dV = a^2 rh1 dx1x dx1y dz(k); FP64, in a fixed reduction order.  No

@@ -109,6 +109,7 @@ SIGNATURES = {
     "pcom_gpu_global_sums": (C.c_int, [C.c_void_p, dbl_p]),
     "pcom_gpu_set_trop_kernel": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_set_overlap": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcom_gpu_set_wait_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "pcom_gpu_set_forcing_async": (C.c_int, [C.c_void_p, C.POINTER(Forcing)]),
     "pcom_gpu_get_state_async": (C.c_int, [C.c_void_p, C.POINTER(State)]),
     "pcom_gpu_set_forcing_months": (C.c_int, [C.c_void_p, C.POINTER(Forcing)]),

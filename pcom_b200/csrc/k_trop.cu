@@ -39,9 +39,10 @@ __device__ bool grid_barrier(const Dev &P, unsigned nblocks) {
         cnt.store(0u, cuda::memory_order_relaxed);
         gen.fetch_add(1u, cuda::memory_order_release);
       } else {
+        const unsigned long long t0 = global_ns();
         long long it = 0;
         while (gen.load(cuda::memory_order_acquire) == g) {
-          if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
+          if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0 || global_ns() - t0 > P.wait_ns) {
             err.store(1, cuda::memory_order_relaxed);
             fail = 1;
             break;
@@ -938,20 +939,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
     __syncthreads();
     if (tid == 0) {
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*bar_cnt);
-      cuda::atomic_ref<int, cuda::thread_scope_device> err(bar_err[0]);
       c.fetch_add(1ULL, cuda::memory_order_release);
       const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
-      long long it = 0;
-      int stop = 0;
-      while (c.load(cuda::memory_order_acquire) < want) {
-        if (++it > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
-          err.store(1, cuda::memory_order_relaxed);
-          stop = 1;
-          break;
-        }
-        if (it > 1024) __nanosleep(32);
-      }
-      s_stop = stop;
+      s_stop = wait_count(bar_cnt, want, bar_err, P.wait_ns) ? 0 : 1;
     }
     __syncthreads();
     if (s_stop) return;

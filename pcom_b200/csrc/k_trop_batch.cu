@@ -18,7 +18,6 @@
 
 namespace {
 
-constexpr long long kSpin = 1LL << 26;
 
 enum {
   B_CH, B_UB, B_VB, B_S1, B_X2, B_PRED, B_SCHE,
@@ -27,25 +26,14 @@ enum {
   B_COUNT
 };
 
-__device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, int *err) {
+__device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, int *err, unsigned long long limit_ns) {
   __syncthreads();
   __shared__ int s_fail;
   if (threadIdx.x == 0) {
     // release: cumulative over the CTA's writes ordered before it by bar.sync
     cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*cnt);
-    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     c.fetch_add(1ULL, cuda::memory_order_release);
-    long long it = 0;
-    int f = 0;
-    while (c.load(cuda::memory_order_acquire) < want) {
-      if (++it > kSpin || e.load(cuda::memory_order_relaxed) != 0) {
-        e.store(1, cuda::memory_order_relaxed);
-        f = 1;
-        break;
-      }
-      if (it > 1024) __nanosleep(32);
-    }
-    s_fail = f;
+    s_fail = wait_count(cnt, want, err, limit_ns) ? 0 : 1;
   }
   __syncthreads();
   return s_fail == 0;
@@ -262,7 +250,7 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
 #undef PT
       __syncthreads();
     }
-    if (!batch_barrier(cnt, (unsigned long long)nt * gridDim.x, err)) return;
+    if (!batch_barrier(cnt, (unsigned long long)nt * gridDim.x, err, Ps[0].wait_ns)) return;
   }
 
   // averages (mod_int.f90:276-288)

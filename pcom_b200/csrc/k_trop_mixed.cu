@@ -19,7 +19,6 @@
 
 namespace {
 
-constexpr long long kSpin = 1LL << 26;
 constexpr int kThreads = 640;
 
 enum { D_CH, D_PRED, D_CN, D_CE, D_COUNT };  // FP64 region fields
@@ -262,20 +261,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     if (tid == 0) {
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*P.tile_flag);
-      cuda::atomic_ref<int, cuda::thread_scope_device> err(P.err[0]);
       c.fetch_add(1ULL, cuda::memory_order_release);
       const unsigned long long want = epoch + (unsigned long long)nt * gridDim.x;
-      long long it = 0;
-      int stop = 0;
-      while (c.load(cuda::memory_order_acquire) < want) {
-        if (++it > kSpin || err.load(cuda::memory_order_relaxed) != 0) {
-          err.store(1, cuda::memory_order_relaxed);
-          stop = 1;
-          break;
-        }
-        if (it > 1024) __nanosleep(32);
-      }
-      s_stop = stop;
+      s_stop = wait_count(P.tile_flag, want, P.err, P.wait_ns) ? 0 : 1;
     }
     __syncthreads();
     if (s_stop) return;

@@ -19,6 +19,7 @@
 #pragma once
 #include <cstdint>
 #include <type_traits>
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #define PCOM_MAXK 64
@@ -68,6 +69,9 @@ struct DevCommon {
   unsigned *bar;   // [0] arrival count, [1] generation
   unsigned long long *tile_flag;  // per-tile progress of the barotropic kernel (monotone across launches)
   int *err;        // [0] timeout flag, [1] watchdog flag
+  // longest a device-side wait (the barotropic kernels' grid barriers) may
+  // take before it gives up and sets err[0] (ns of global time)
+  unsigned long long wait_ns = 2000000000ULL;
   // lat-lon (separable) metrics: dx?x depends on i only, dx?y and rh? on j
   // only (set_hgrid builds them from 1-D lon/lat, main.f90:408-493); when the
   // uploaded 2-D arrays have that structure these 1-D copies are set
@@ -130,6 +134,32 @@ PD int IP(const DevT<R> &P, int i) { return i == P.ni - 1 ? 2 : i + 1; }
 
 PD double ld(const double *p, long long q) { return __ldg(p + q); }
 PD float ld(const float *p, long long q) { return __ldg(p + q); }
+
+// global time in ns
+PD unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// One thread's bounded wait for an arrival counter to reach `want`: gives up
+// when another thread has set *err, or after limit_ns of global time (then
+// it sets *err itself; an iteration cap bounds the loop as well).  Returns
+// true when the counter got there.
+PD bool wait_count(unsigned long long *cnt, unsigned long long want, int *err, unsigned long long limit_ns) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*cnt);
+  cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+  if (c.load(cuda::memory_order_acquire) >= want) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long it = 1; it < (1LL << 28); ++it) {
+    if (c.load(cuda::memory_order_acquire) >= want) return true;
+    if (e.load(cuda::memory_order_relaxed) != 0) return false;
+    if (global_ns() - t0 > limit_ns) break;
+    if (it > 1024) __nanosleep(32);
+  }
+  e.store(1, cuda::memory_order_relaxed);
+  return false;
+}
 
 // x / y rounded to nearest, given ry = 1/y correctly rounded: the quotient
 // estimate x*ry is corrected once with its exact remainder (Markstein's

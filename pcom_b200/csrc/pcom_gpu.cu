@@ -1613,6 +1613,15 @@ int pcom_gpu_set_trop_kernel(pcom_handle *h, int32_t which) {
   return PCOM_OK;
 }
 
+int pcom_gpu_set_wait_limit(pcom_handle *h, double seconds) {
+  if (!h) return fail(PCOM_ERR_ARG, "null handle");
+  if (!(seconds >= 0.0) || seconds > 1.0e6) return fail(PCOM_ERR_ARG, "wait limit must be in [0, 1e6] s");
+  CK(cudaStreamSynchronize(h->stream));
+  h->D.wait_ns = (unsigned long long)(seconds * 1.0e9);
+  sync_common(h);
+  return PCOM_OK;
+}
+
 int pcom_gpu_set_overlap(pcom_handle *h, int32_t enable) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(h->stream));
