@@ -136,31 +136,11 @@ class Clocks:
 
 # --------------------------------------------------------------- roofline
 def algorithmic_bytes(kernel: str, glo_ni: int, glo_nj: int, nk: int, nstep: int) -> float:
-    """Bytes a kernel must move per launch at minimum (FP64, wet or not).
+    """Bytes a kernel must move per launch at minimum on the FP64 path (the
+    per-kernel field counts of pcom_b200.roofline)."""
+    from pcom_b200.roofline import algorithmic_bytes as ab
 
-    3-D fields count glo_ni*glo_nj*nk points, 2-D fields glo_ni*glo_nj.  The
-    per-kernel field counts are the reads/writes listed in DESIGN.md."""
-    n2 = glo_ni * glo_nj
-    n3 = n2 * nk
-    s = 8.0
-    table = {
-        # kernel: (3-D fields read+written, 2-D fields read+written)
-        "den_alpha+int_tobot": (4, 1),         # R tc, sc; W alpha, adp; R chc
-        "int_pgra": (2, 8 + 4),                # R alpha, adp; W bphi/bgraphi (8); statics
-        "readyc_2d": (0, 4 + 6),
-        "upwelling": (3, 4),                   # R uc, vc; W wm
-        "readyc_3d": (2 + 1 + 2 + 4 + 1, 6),   # R uc, vc, wm, am, (km); W auc, avc, fx, fy
-        "int_trop": (0, nstep * 6 + 30),       # per substep R/W ch, ub, vb; statics once
-        "int_clin": (12 + 7, 8),               # R adp, alpha, 6 AB3, fx, fy, uc, vc, up, vp; W uc, vc, up, vp, uu, vv, acu
-        "smag": (3, 2),
-        "int_ssh": (3, 3),
-        "ts_2d": (0, 4),
-        "upwelling+acw": (6, 4),
-        "int_ts": (4 + 2 + 1 + 2 + 1 + 2 + 6, 6),  # R tc, sc, tp, sp, uc, vc, wm, kh, prho(2); W tn, sn; RW act, acs, acr
-        "den_prho": (4, 1),
-    }
-    f3, f2 = table.get(kernel, (0, 0))
-    return s * (f3 * n3 + f2 * n2)
+    return ab(kernel, glo_ni, glo_nj, nk, nstep, mixed=False)
 
 
 def run_ours(args):
