@@ -679,10 +679,16 @@ int trop_res_max_blocks(int TX, int TY) {
 // (ensemble members, basins), one tile per CTA; each CTA reads its domain's
 // Dev from `Ps`, and the grid barrier counts on `gcnt` (zeroed before the
 // launch) with timeouts flagged in `gerr`.
-template <bool GROUP>
+//
+// CTX, CTY > 0: the same kernel compiled for one tile shape, so that the
+// region's row length and plane size are constants and every shared-memory
+// operand is a fixed offset from the thread's own point (fewer instructions
+// and registers per substep than the general form, CTX = CTY = 0).
+template <bool GROUP, int CTX = 0, int CTY = 0>
 __global__ void __launch_bounds__(kResThreads, 1)
     k_trop_fast(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps, const TileRef *__restrict__ tiles,
                 int TX, int TY, int ntx, unsigned long long epoch, unsigned long long *gcnt, int *gerr) {
+  if (CTX > 0) { TX = CTX; TY = CTY; }
   extern __shared__ double sm[];
   __shared__ int s_stop;
   const TileRef T = GROUP ? tiles[blockIdx.x] : TileRef{0, 0, 0, 0, 0};
@@ -966,10 +972,20 @@ size_t trop_fast_smem_bytes(int TX, int TY) {
   return ((size_t)R_COUNT * (TX + 4) * (TY + 4) + 8 * (TX + 4) + 19 * (TY + 4)) * sizeof(double);
 }
 
+namespace {
+// the single-domain kernel for a tile shape: the fixed-shape form where one
+// is compiled (the 24 x 18 tiles of the 1-degree 360 x 160 domain)
+const void *fast_kernel(int TX, int TY) {
+  if (TX == 24 && TY == 18) return (const void *)k_trop_fast<false, 24, 18>;
+  return (const void *)k_trop_fast<false>;
+}
+}  // namespace
+
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
   const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  cudaError_t e = cudaFuncSetAttribute(k_trop_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const void *fn = fast_kernel(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
   const Dev *nps = nullptr;
@@ -978,7 +994,7 @@ cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long ep
   int *nerr = nullptr;
   void *args[] = {(void *)&P, (void *)&nps, (void *)&nts, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch,
                   (void *)&ncnt, (void *)&nerr};
-  return cudaLaunchCooperativeKernel((const void *)k_trop_fast<false>, dim3(ntx * nty), dim3(nthreads), args, smem, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(ntx * nty), dim3(nthreads), args, smem, s);
 }
 
 namespace {
@@ -989,10 +1005,10 @@ int fast_max_blocks(int TX, int TY) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  if (cudaFuncSetAttribute(k_trop_fast<GROUP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return 0;
+  const void *fn = GROUP ? (const void *)k_trop_fast<true> : fast_kernel(TX, TY);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_fast<GROUP>, nthreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, nthreads, smem) != cudaSuccess) return 0;
   return per * nsm;
 }
 }  // namespace

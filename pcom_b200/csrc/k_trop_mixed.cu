@@ -30,8 +30,12 @@ constexpr int kVx = 8, kVy = 19;  // FP32 metric vectors over lx and ly
 
 }  // namespace
 
+// CTX, CTY > 0: compiled for one tile shape (constant region strides, as in
+// k_trop_fast); CTX = CTY = 0: any shape
+template <int CTX = 0, int CTY = 0>
 __global__ void __launch_bounds__(kThreads, 1)
     k_trop_mixed(const __grid_constant__ Dev P, int TX, int TY, int ntx, unsigned long long epoch) {
+  if (CTX > 0) { TX = CTX; TY = CTY; }
   extern __shared__ double smd[];
   __shared__ int s_stop;
   const int nj = P.nj, njm = P.njm, ni = P.ni, G = P.glo_ni;
@@ -285,6 +289,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   (void)btd;
 }
 
+namespace {
+// the fixed-shape form for the 24 x 18 tiles of the 1-degree 360 x 160 domain
+const void *mixed_kernel(int TX, int TY) {
+  if (TX == 24 && TY == 18) return (const void *)k_trop_mixed<24, 18>;
+  return (const void *)k_trop_mixed<>;
+}
+}  // namespace
+
 size_t trop_mixed_smem_bytes(int TX, int TY) {
   const size_t rs = (size_t)(TX + 4) * (TY + 4);
   return D_COUNT * rs * sizeof(double) + (F_COUNT * rs + kVx * (TX + 4) + kVy * (TY + 4)) * sizeof(float);
@@ -296,18 +308,20 @@ int trop_mixed_max_blocks(int TX, int TY) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_mixed_smem_bytes(TX, TY);
-  if (cudaFuncSetAttribute(k_trop_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  const void *fn = mixed_kernel(TX, TY);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_mixed, nthreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, nthreads, smem) != cudaSuccess) return 0;
   return per * nsm;
 }
 
 cudaError_t launch_trop_mixed(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
   const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
   const size_t smem = trop_mixed_smem_bytes(TX, TY);
-  cudaError_t e = cudaFuncSetAttribute(k_trop_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const void *fn = mixed_kernel(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
   void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch};
-  return cudaLaunchCooperativeKernel((const void *)k_trop_mixed, dim3(ntx * nty), dim3(nthreads), args, smem, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(ntx * nty), dim3(nthreads), args, smem, s);
 }
