@@ -41,18 +41,28 @@ __device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, 
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, const TileRef *__restrict__ tiles,
-                                                    int ntiles, int TX, int TY, unsigned long long *cnt, int *err) {
+// SINGLE: every tile belongs to one domain, passed by value (P0, read through
+// the constant cache); otherwise each tile's domain is Ps[tile.m].
+// CTX, CTY > 0: compiled for one tile shape, so the region strides and the
+// stage loops' point -> (lx, ly) divisions are constants; each stage walks
+// the rectangle a full tile would cover and skips points outside its part
+// of a partial tile.
+template <bool SINGLE, int CTX = 0, int CTY = 0>
+__global__ void __launch_bounds__(256) k_trop_batch(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps,
+                                                    const TileRef *__restrict__ tiles, int ntiles, int TX, int TY,
+                                                    unsigned long long *cnt, int *err) {
+  if (CTX > 0) { TX = CTX; TY = CTY; }
   extern __shared__ double sm[];
   const int W = TX + 4, RS = W * (TY + 4);
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int nstep = Ps[0].nstep;
+  const int nstep = SINGLE ? P0.nstep : Ps[0].nstep;
+  const unsigned long long wait_ns = SINGLE ? P0.wait_ns : Ps[0].wait_ns;
   auto S = [&](int f, int p) -> double & { return sm[f * RS + p]; };
 
   // accumulators of owned points (mod_int.f90:176-180)
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileRef T = tiles[t];
-    const Dev &P = Ps[T.m];
+    const Dev &P = SINGLE ? P0 : Ps[T.m];
     for (int p = tid; p < T.tw * T.th; p += nth) {
       const int i = T.r0 + p % T.tw + 2, j = T.j0 + p / T.tw;
       const long long q = I2(P, i, j);
@@ -67,7 +77,7 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
     const int d = (nt - 1) & 1;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       const TileRef T = tiles[t];
-      const Dev &P = Ps[T.m];
+      const Dev &P = SINGLE ? P0 : Ps[T.m];
       const int G = P.glo_ni, nj = P.nj, njm = P.njm, ni = P.ni;
       const int tw = T.tw, th = T.th, rr0 = T.r0 - 2, jj0 = T.j0 - 2;
       const double a = P.c.a, ra = P.ra, bt = (double)P.bt, gamma_b = P.c.gamma_b;
@@ -75,25 +85,30 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
       const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
       const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
       auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
-      // region point p -> (lx, ly, i, j, q); valid rows only
-#define PT(nx, lo_x, lo_y)                                  \
-  const int lx = (lo_x) + pp % (nx), ly = (lo_y) + pp / (nx); \
-  const int j = jj0 + ly;                                   \
-  if (j < 1 || j > nj) continue;                            \
-  const int i = ring_i(rr0 + lx);                           \
-  const long long q = I2(P, i, j);                          \
-  const int p = ly * W + lx;                                \
+      // stage loop over the (TX + e) x (TY + e) rectangle from (lo_x, lo_y)
+      // that a full tile's stage covers; region point -> (lx, ly, i, j, q),
+      // points outside this tile's (tw + e) x (th + e) part and invalid rows
+      // skipped
+#define STAGE(e) for (int pp = tid; pp < (TX + (e)) * (TY + (e)); pp += nth)
+#define PT(e, lo_x, lo_y)                                                   \
+  const int lx = (lo_x) + pp % (TX + (e)), ly = (lo_y) + pp / (TX + (e));   \
+  if (lx >= (lo_x) + tw + (e) || ly >= (lo_y) + th + (e)) continue;         \
+  const int j = jj0 + ly;                                                   \
+  if (j < 1 || j > nj) continue;                                            \
+  const int i = ring_i(rr0 + lx);                                           \
+  const long long q = I2(P, i, j);                                          \
+  const int p = ly * W + lx;                                                \
   (void)i;
       // S1: previous state (L2 loads: written by other CTAs)
-      for (int pp = tid; pp < (tw + 4) * (th + 4); pp += nth) {
-        PT(tw + 4, 0, 0)
+      STAGE(4) {
+        PT(4, 0, 0)
         S(B_CH, p) = __ldcg(src_ch + q);
         if (lx < tw + 3 && ly < th + 3) { S(B_UB, p) = __ldcg(src_ub + q); S(B_VB, p) = __ldcg(src_vb + q); }
       }
       __syncthreads();
       // S2: sch = sqrt(ter(ch)) on U, supb
-      for (int pp = tid; pp < (tw + 3) * (th + 3); pp += nth) {
-        PT(tw + 3, 0, 0)
+      STAGE(3) {
+        PT(3, 0, 0)
         double sch = 1.0;
         if (__ldg(P.lev_u + q) > 0) {
           const double w = (j <= njm) ? (S(B_CH, p) + S(B_CH, p + W) + S(B_CH, p + 1) + S(B_CH, p + W + 1)) * 0.25 : 0.0;
@@ -105,8 +120,8 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
       }
       __syncthreads();
       // S4: predictor ch
-      for (int pp = tid; pp < (tw + 2) * (th + 2); pp += nth) {
-        PT(tw + 2, 1, 1)
+      STAGE(2) {
+        PT(2, 1, 1)
         const bool srow = j >= 2;
         const double tEc = srow ? 0.5 * (S(B_S1, p - W) + S(B_S1, p)) : 0.0;
         const double tEw = srow ? 0.5 * (S(B_S1, p - W - 1) + S(B_S1, p - 1)) : 0.0;
@@ -125,8 +140,8 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
       }
       __syncthreads();
       // S5: sch on U, N- and E-grid intermediates
-      for (int pp = tid; pp < (tw + 2) * (th + 2); pp += nth) {
-        PT(tw + 2, 1, 1)
+      STAGE(2) {
+        PT(2, 1, 1)
         const bool nrow = j <= njm, srow = j >= 2;
         const bool inU = lx < tw + 2 && ly < th + 2, inN = ly < th + 2, inE = lx < tw + 2;
         if (inU) {
@@ -167,8 +182,8 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
       }
       __syncthreads();
       // S6: corrector velocity
-      for (int pp = tid; pp < (tw + 1) * (th + 1); pp += nth) {
-        PT(tw + 1, 1, 1)
+      STAGE(1) {
+        PT(1, 1, 1)
         const bool nrow = j <= njm;
         const double seau = (double)(__ldg(P.lev_u + q) >= 1);
         const double rh3 = __ldg(P.rh1d[3] + j - 1);
@@ -223,8 +238,8 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
       }
       __syncthreads();
       // S8: corrector ch on the tile, store, accumulate
-      for (int pp = tid; pp < tw * th; pp += nth) {
-        PT(tw, 2, 2)
+      STAGE(0) {
+        PT(0, 2, 2)
         const bool srow = j >= 2;
         const double tEc = srow ? 0.5 * (S(B_S1, p - W) + S(B_S1, p)) : 0.0;
         const double tEw = srow ? 0.5 * (S(B_S1, p - W - 1) + S(B_S1, p - 1)) : 0.0;
@@ -248,15 +263,16 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
         P.tr_acc[3][q] = P.tr_acc[3][q] + vbc;
       }
 #undef PT
+#undef STAGE
       __syncthreads();
     }
-    if (!batch_barrier(cnt, (unsigned long long)nt * gridDim.x, err, Ps[0].wait_ns)) return;
+    if (!batch_barrier(cnt, (unsigned long long)nt * gridDim.x, err, wait_ns)) return;
   }
 
   // averages (mod_int.f90:276-288)
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileRef T = tiles[t];
-    const Dev &P = Ps[T.m];
+    const Dev &P = SINGLE ? P0 : Ps[T.m];
     for (int p = tid; p < T.tw * T.th; p += nth) {
       const int i = T.r0 + p % T.tw + 2, j = T.j0 + p / T.tw;
       const long long q = I2(P, i, j);
@@ -275,26 +291,56 @@ __global__ void __launch_bounds__(256) k_trop_batch(const Dev *__restrict__ Ps, 
   }
 }
 
+namespace {
+// the form for a tile shape: the fixed-shape one for the 32 x 8 tiles the
+// single-domain selector uses, the general one otherwise
+template <bool SINGLE>
+const void *batch_kernel(int TX, int TY) {
+  if (TX == 32 && TY == 8) return (const void *)k_trop_batch<SINGLE, 32, 8>;
+  return (const void *)k_trop_batch<SINGLE>;
+}
+}  // namespace
+
 size_t trop_batch_smem(int TX, int TY) { return (size_t)B_COUNT * (TX + 4) * (TY + 4) * sizeof(double); }
 
+// co-resident CTAs of the multi-tile kernel for a tile shape (the smaller of
+// its single-domain and batched forms)
 int trop_batch_max_blocks(int TX, int TY) {
-  int dev = 0, nsm = 0, per = 0;
+  int dev = 0, nsm = 0, best = 1 << 30;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_batch_smem(TX, TY);
-  if (cudaFuncSetAttribute(k_trop_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trop_batch, 256, smem) != cudaSuccess) return 0;
-  return per * nsm;
+  for (const void *fn : {batch_kernel<true>(TX, TY), batch_kernel<false>(TX, TY)}) {
+    int per = 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem) != cudaSuccess) return 0;
+    best = per < best ? per : best;
+  }
+  return best * nsm;
 }
 
-cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
-                              unsigned long long *cnt, int *err, cudaStream_t s) {
+namespace {
+cudaError_t launch_batch_form(const void *fn, const Dev &P0, const Dev *dPs, const TileRef *dtiles, int ntiles, int TX,
+                              int TY, int nblocks, unsigned long long *cnt, int *err, cudaStream_t s) {
   const size_t smem = trop_batch_smem(TX, TY);
-  cudaError_t e = cudaFuncSetAttribute(k_trop_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // the barrier counter starts from zero in every launch
   e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  void *args[] = {(void *)&dPs, (void *)&dtiles, (void *)&ntiles, (void *)&TX, (void *)&TY, (void *)&cnt, (void *)&err};
-  return cudaLaunchCooperativeKernel((const void *)k_trop_batch, dim3(nblocks), dim3(256), args, smem, s);
+  void *args[] = {(void *)&P0, (void *)&dPs, (void *)&dtiles, (void *)&ntiles, (void *)&TX, (void *)&TY,
+                  (void *)&cnt, (void *)&err};
+  return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(256), args, smem, s);
+}
+}  // namespace
+
+cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
+                              unsigned long long *cnt, int *err, cudaStream_t s) {
+  const Dev none{};
+  return launch_batch_form(batch_kernel<false>(TX, TY), none, dPs, dtiles, ntiles, TX, TY, nblocks, cnt, err, s);
+}
+
+cudaError_t launch_trop_multi(const Dev &P, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
+                              unsigned long long *cnt, int *err, cudaStream_t s) {
+  return launch_batch_form(batch_kernel<true>(TX, TY), P, nullptr, dtiles, ntiles, TX, TY, nblocks, cnt, err, s);
 }

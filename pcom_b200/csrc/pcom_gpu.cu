@@ -197,13 +197,6 @@ __global__ void k_int_bnd(const double *frc, double *taux, double *tauy, double 
   }
 }
 
-// stream-ordered copy of a Dev (kernel parameter) to device memory
-__global__ void k_copy_dev(const __grid_constant__ Dev P, Dev *out) {
-  const int n = (int)(sizeof(Dev) / sizeof(int));
-  const int *src = reinterpret_cast<const int *>(&P);
-  int *dst = reinterpret_cast<int *>(out);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-}
 
 // ---- closure coupling (FP64 handles)
 struct Grid2 {
@@ -352,10 +345,9 @@ struct pcom_handle {
   int trop_tx = 24, trop_ty = 18, trop_blocks = 0;
   bool trop_resident = false;
   // domains too large for the resident kernel: the multi-tile kernel over
-  // this domain's tile list (its Dev copied to the device per launch)
+  // this domain's tile list (its Dev passed by value per launch)
   bool trop_multi = false;
   int trop_force = 0;  // 0 automatic, 1 resident, 2 multi-tile, 3 generic
-  Dev *d_dev1 = nullptr;
   TileRef *d_tiles1 = nullptr;
   int ntiles1 = 0;
   unsigned long long *d_cnt1 = nullptr;
@@ -512,9 +504,8 @@ int pick_trop_config(pcom_handle *h) {
       const int G = h->dims.glo_ni, nj = h->nj;
       for (int j0 = 1; j0 <= nj; j0 += ty)
         for (int r0 = 0; r0 < G; r0 += tx) t.push_back({0, r0, j0, std::min(tx, G - r0), std::min(ty, nj - j0 + 1)});
-      if (!h->d_dev1) {
-        int rc = h->alloc(&h->d_dev1, 1);
-        if (!rc) rc = h->alloc(&h->d_cnt1, 1);
+      if (!h->d_cnt1) {
+        int rc = h->alloc(&h->d_cnt1, 1);
         if (rc) return rc;
       }
       int rc = h->alloc(&h->d_tiles1, t.size());
@@ -620,11 +611,8 @@ int do_trop(pcom_handle *h) {
       e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
   } else if (h->trop_multi) {
-    k_copy_dev<<<1, 256, 0, h->stream>>>(h->D, h->d_dev1);
-    e = cudaGetLastError();
-    if (e == cudaSuccess)
-      e = launch_trop_batch(h->d_dev1, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1,
-                            h->D.err, h->stream);
+    e = launch_trop_multi(h->D, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1, h->D.err,
+                          h->stream);
   } else {
     e = launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
   }

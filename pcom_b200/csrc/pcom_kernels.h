@@ -58,6 +58,9 @@ size_t trop_batch_smem(int TX, int TY);
 int trop_batch_max_blocks(int TX, int TY);
 cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
                               unsigned long long *cnt, int *err, cudaStream_t s);
+// the same kernel over the tiles of one domain P (passed by value)
+cudaError_t launch_trop_multi(const Dev &P, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
+                              unsigned long long *cnt, int *err, cudaStream_t s);
 // resident form: one tile per CTA, coefficients in registers (the fast
 // kernel over a tile list); all tiles of the group must be co-resident
 int trop_group_max_blocks(int TX, int TY);
