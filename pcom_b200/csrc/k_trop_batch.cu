@@ -47,8 +47,13 @@ __device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, 
 // stage loops' point -> (lx, ly) divisions are constants; each stage walks
 // the rectangle a full tile would cover and skips points outside its part
 // of a partial tile.
+// Threads per CTA: 512 for one domain (40 registers: a region point per
+// thread for 32 x 8 tiles), 256 for a batch (more registers per thread).
+template <bool SINGLE>
+constexpr int batch_threads() { return SINGLE ? 512 : 256; }
+
 template <bool SINGLE, int CTX = 0, int CTY = 0>
-__global__ void __launch_bounds__(256) k_trop_batch(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps,
+__global__ void __launch_bounds__(batch_threads<SINGLE>()) k_trop_batch(const __grid_constant__ Dev P0, const Dev *__restrict__ Ps,
                                                     const TileRef *__restrict__ tiles, int ntiles, int TX, int TY,
                                                     unsigned long long *cnt, int *err) {
   if (CTX > 0) { TX = CTX; TY = CTY; }
@@ -310,18 +315,21 @@ int trop_batch_max_blocks(int TX, int TY) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_batch_smem(TX, TY);
-  for (const void *fn : {batch_kernel<true>(TX, TY), batch_kernel<false>(TX, TY)}) {
+  const void *fns[2] = {batch_kernel<true>(TX, TY), batch_kernel<false>(TX, TY)};
+  const int nth[2] = {batch_threads<true>(), batch_threads<false>()};
+  for (int f = 0; f < 2; ++f) {
     int per = 0;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fns[f], nth[f], smem) != cudaSuccess) return 0;
     best = per < best ? per : best;
   }
   return best * nsm;
 }
 
 namespace {
-cudaError_t launch_batch_form(const void *fn, const Dev &P0, const Dev *dPs, const TileRef *dtiles, int ntiles, int TX,
-                              int TY, int nblocks, unsigned long long *cnt, int *err, cudaStream_t s) {
+cudaError_t launch_batch_form(const void *fn, int nthreads, const Dev &P0, const Dev *dPs, const TileRef *dtiles,
+                              int ntiles, int TX, int TY, int nblocks, unsigned long long *cnt, int *err,
+                              cudaStream_t s) {
   const size_t smem = trop_batch_smem(TX, TY);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -330,17 +338,19 @@ cudaError_t launch_batch_form(const void *fn, const Dev &P0, const Dev *dPs, con
   if (e != cudaSuccess) return e;
   void *args[] = {(void *)&P0, (void *)&dPs, (void *)&dtiles, (void *)&ntiles, (void *)&TX, (void *)&TY,
                   (void *)&cnt, (void *)&err};
-  return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(256), args, smem, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(nthreads), args, smem, s);
 }
 }  // namespace
 
 cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
                               unsigned long long *cnt, int *err, cudaStream_t s) {
   const Dev none{};
-  return launch_batch_form(batch_kernel<false>(TX, TY), none, dPs, dtiles, ntiles, TX, TY, nblocks, cnt, err, s);
+  return launch_batch_form(batch_kernel<false>(TX, TY), batch_threads<false>(), none, dPs, dtiles, ntiles, TX, TY,
+                           nblocks, cnt, err, s);
 }
 
 cudaError_t launch_trop_multi(const Dev &P, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,
                               unsigned long long *cnt, int *err, cudaStream_t s) {
-  return launch_batch_form(batch_kernel<true>(TX, TY), P, nullptr, dtiles, ntiles, TX, TY, nblocks, cnt, err, s);
+  return launch_batch_form(batch_kernel<true>(TX, TY), batch_threads<true>(), P, nullptr, dtiles, ntiles, TX, TY,
+                           nblocks, cnt, err, s);
 }
