@@ -47,8 +47,8 @@ __device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, 
 // stage loops' point -> (lx, ly) divisions are constants; each stage walks
 // the rectangle a full tile would cover and skips points outside its part
 // of a partial tile.
-// Threads per CTA: 512 for one domain (40 registers: a region point per
-// thread for 32 x 8 tiles), 256 for a batch (more registers per thread).
+// Threads per CTA: 512 for one domain (about 40 registers: a region point
+// per thread for 32 x 10 tiles), 256 for a batch (more registers per thread).
 template <bool SINGLE>
 constexpr int batch_threads() { return SINGLE ? 512 : 256; }
 
@@ -297,11 +297,12 @@ __global__ void __launch_bounds__(batch_threads<SINGLE>()) k_trop_batch(const __
 }
 
 namespace {
-// the form for a tile shape: the fixed-shape one for the 32 x 8 tiles the
-// single-domain selector uses, the general one otherwise
+// the form for a tile shape: the fixed-shape one for the 32 x 10 tiles the
+// single-domain selector uses (a 36 x 14 region: 504 of the 512 threads), the
+// general one otherwise
 template <bool SINGLE>
 const void *batch_kernel(int TX, int TY) {
-  if (TX == 32 && TY == 8) return (const void *)k_trop_batch<SINGLE, 32, 8>;
+  if (SINGLE && TX == 32 && TY == 10) return (const void *)k_trop_batch<true, 32, 10>;
   return (const void *)k_trop_batch<SINGLE>;
 }
 }  // namespace

@@ -497,7 +497,7 @@ int pick_trop_config(pcom_handle *h) {
   // coefficients from L2) over this domain's tiles
   if (h->trop_force == 1) return fail(PCOM_ERR_ARG, "the domain does not fit the resident barotropic kernel");
   if (h->D.separable && (h->trop_force == 0 || h->trop_force == 2)) {
-    const int tx = 32, ty = 8;
+    const int tx = 32, ty = 10;
     const int mb = trop_batch_max_blocks(tx, ty);
     if (mb > 0) {
       std::vector<TileRef> t;
