@@ -26,6 +26,8 @@ enum {
   B_COUNT
 };
 
+__device__ __forceinline__ void prefetch_l2(const void *a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+
 __device__ bool batch_barrier(unsigned long long *cnt, unsigned long long want, int *err, unsigned long long limit_ns) {
   __syncthreads();
   __shared__ int s_fail;
@@ -104,11 +106,20 @@ __global__ void __launch_bounds__(batch_threads<SINGLE>()) k_trop_batch(const __
   const long long q = I2(P, i, j);                                          \
   const int p = ly * W + lx;                                                \
   (void)i;
-      // S1: previous state (L2 loads: written by other CTAs)
+      // S1: previous state (L2 loads: written by other CTAs).  The 2-D
+      // fields the later stages read at this point are prefetched into L2
+      // (the substep's working set is larger than L2, so they would otherwise
+      // come from HBM one stage at a time)
       STAGE(4) {
         PT(4, 0, 0)
         S(B_CH, p) = __ldcg(src_ch + q);
         if (lx < tw + 3 && ly < th + 3) { S(B_UB, p) = __ldcg(src_ub + q); S(B_VB, p) = __ldcg(src_vb + q); }
+        prefetch_l2(P.lev_u + q); prefetch_l2(P.lev_t + q);
+        prefetch_l2(P.prh_u + q); prefetch_l2(P.prh_t + q); prefetch_l2(P.rprh_t + q);
+        prefetch_l2(P.am + q); prefetch_l2(P.rwt + q); prefetch_l2(P.cor + q);
+        prefetch_l2(P.ut + q); prefetch_l2(P.vt + q); prefetch_l2(P.graphihx + q); prefetch_l2(P.graphihy + q);
+        for (int f = 0; f < 4; ++f) { prefetch_l2(P.bphi[f] + q); prefetch_l2(P.bgra[f] + q); }
+        for (int f = 0; f < 6; ++f) prefetch_l2(P.tr_acc[f] + q);
       }
       __syncthreads();
       // S2: sch = sqrt(ter(ch)) on U, supb
