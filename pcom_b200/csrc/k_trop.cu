@@ -785,6 +785,21 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const double land_ch0 = inS4 ? P.chc[q] : 0.0;
   __syncthreads();
 
+  // S2 at this thread's point: sch = sqrt(ter(ch)) on U and the fluxes
+  // supb.  Points with lx in 2..tw and ly in 2..th read only the tile's own
+  // state (ch at the point and its E, N, NE neighbours; ub, vb at the point)
+  auto s2 = [&]() {
+    double sch = 1.0;
+    if (levu > 0) {
+      const double w = nrow ? (S(R_CH, p) + S(R_CH, p + W) + S(R_CH, p + 1) + S(R_CH, p + W + 1)) * 0.25 : 0.0;
+      sch = sqrt(w);
+    }
+    const double ps = prh_u * sch;
+    S(R_S1, p) = ps * S(R_UB, p);
+    S(R_X2, p) = ps * S(R_VB, p) * RH(3, ly);
+  };
+  const bool s2own = inS2 && lx >= 2 && lx <= tw && ly >= 2 && ly <= th;
+
   const unsigned long long base = epoch;  // arrivals counted before this launch
   for (int nt = 1; nt <= nstep; ++nt) {
     const int d = (nt - 1) & 1;
@@ -799,17 +814,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
       if (inS2) { S(R_UB, p) = __ldcg(src_ub + q); S(R_VB, p) = __ldcg(src_vb + q); }
     }
     __syncthreads();
-    // S2: sch = sqrt(ter(ch)) on U, supb
-    if (inS2) {
-      double sch = 1.0;
-      if (levu > 0) {
-        const double w = nrow ? (S(R_CH, p) + S(R_CH, p + W) + S(R_CH, p + 1) + S(R_CH, p + W + 1)) * 0.25 : 0.0;
-        sch = sqrt(w);
-      }
-      const double ps = prh_u * sch;
-      S(R_S1, p) = ps * S(R_UB, p);
-      S(R_X2, p) = ps * S(R_VB, p) * RH(3, ly);
-    }
+    // S2: sch = sqrt(ter(ch)) on U, supb (after the first substep the
+    // points whose inputs are all the tile's own were done while waiting at
+    // the grid barrier)
+    if (inS2 && (nt == 1 || !s2own)) s2();
     __syncthreads();
     // S4: predictor ch; the ter U->E (rows >= 2) and U->N means of supb are
     // formed here from the staged supb
@@ -942,10 +950,16 @@ __global__ void __launch_bounds__(kResThreads, 1)
     // writes ordered before it by bar.sync), then waits (bounded, acquire)
     // for all arrivals of this substep; the counter is never reset, targets
     // grow per launch.  The outcome reaches the CTA through shared memory.
+    // Between the arrival and the wait the CTA does the next substep's S2 on
+    // the points that need no other tile's state (shared memory only: the
+    // S8 reads of supb are behind the CTA barrier).
     __syncthreads();
     if (tid == 0) {
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*bar_cnt);
       c.fetch_add(1ULL, cuda::memory_order_release);
+    }
+    if (nt < nstep && s2own) s2();
+    if (tid == 0) {
       const unsigned long long want = base + (unsigned long long)nt * gridDim.x;
       s_stop = wait_count(bar_cnt, want, bar_err, P.wait_ns) ? 0 : 1;
     }
