@@ -993,6 +993,18 @@ const void *fast_kernel(int TX, int TY) {
   if (TX == 24 && TY == 18) return (const void *)k_trop_fast<false, 24, 18>;
   return (const void *)k_trop_fast<false>;
 }
+// the group kernel for a tile shape: a fixed-shape form for each tile shape
+// the batch autotuner tries (pcom_gpu_batch_autotune), the general one
+// otherwise
+const void *group_kernel(int TX, int TY) {
+#define PCOM_GROUP_SHAPE(x, y) \
+  if (TX == (x) && TY == (y)) return (const void *)k_trop_fast<true, (x), (y)>;
+  PCOM_GROUP_SHAPE(12, 12) PCOM_GROUP_SHAPE(16, 8) PCOM_GROUP_SHAPE(16, 12) PCOM_GROUP_SHAPE(16, 16)
+  PCOM_GROUP_SHAPE(24, 12) PCOM_GROUP_SHAPE(20, 16) PCOM_GROUP_SHAPE(24, 18) PCOM_GROUP_SHAPE(32, 8)
+  PCOM_GROUP_SHAPE(32, 12) PCOM_GROUP_SHAPE(28, 16) PCOM_GROUP_SHAPE(48, 8) PCOM_GROUP_SHAPE(64, 6)
+#undef PCOM_GROUP_SHAPE
+  return (const void *)k_trop_fast<true>;
+}
 }  // namespace
 
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
@@ -1019,7 +1031,7 @@ int fast_max_blocks(int TX, int TY) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  const void *fn = GROUP ? (const void *)k_trop_fast<true> : fast_kernel(TX, TY);
+  const void *fn = GROUP ? group_kernel(TX, TY) : fast_kernel(TX, TY);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, nthreads, smem) != cudaSuccess) return 0;
@@ -1033,7 +1045,8 @@ int trop_group_max_blocks(int TX, int TY) { return fast_max_blocks<true>(TX, TY)
 cudaError_t launch_trop_group(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY,
                               unsigned long long *cnt, int *err, cudaStream_t s) {
   const size_t smem = trop_fast_smem_bytes(TX, TY);
-  cudaError_t e = cudaFuncSetAttribute(k_trop_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const void *fn = group_kernel(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // the group's barrier counter starts from zero in every launch
   e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
@@ -1044,5 +1057,5 @@ cudaError_t launch_trop_group(const Dev *dPs, const TileRef *dtiles, int ntiles,
   const unsigned long long epoch = 0;
   void *args[] = {(void *)&none, (void *)&dPs, (void *)&dtiles, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch,
                   (void *)&cnt, (void *)&err};
-  return cudaLaunchCooperativeKernel((const void *)k_trop_fast<true>, dim3(ntiles), dim3(nthreads), args, smem, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(ntiles), dim3(nthreads), args, smem, s);
 }
