@@ -38,6 +38,9 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <memory>
+#include <utility>
+#include <malloc.h>
 #include <map>
 #ifdef _OPENMP
 #include <omp.h>
@@ -46,13 +49,30 @@
 namespace {
 
 /* ------------------------------------------------------------------ arrays */
+// Allocator whose resize leaves new doubles/ints uninitialised, so that an
+// array's fill below runs in parallel instead of as a serial zero-fill.
+template <class T>
+struct DefaultInit : std::allocator<T> {
+  template <class U>
+  struct rebind { using other = DefaultInit<U>; };
+  DefaultInit() = default;
+  template <class U>
+  DefaultInit(const DefaultInit<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) noexcept { ::new ((void *)p) U; }
+  template <class U, class... Args>
+  void construct(U *p, Args &&...args) { ::new ((void *)p) U(std::forward<Args>(args)...); }
+};
 struct A3 {
   int n1 = 0, n2 = 0, n3 = 0;
-  std::vector<double> v;
+  std::vector<double, DefaultInit<double>> v;
   A3() {}
   A3(int a, int b, int c = 1, double x = 0.0) { init(a, b, c, x); }
   void init(int a, int b, int c = 1, double x = 0.0) {
-    n1 = a; n2 = b; n3 = c; v.assign((size_t)a * b * c, x);
+    n1 = a; n2 = b; n3 = c;
+    const long long n = (long long)a * b * c;
+    v.resize((size_t)n);
+    _Pragma("omp parallel for schedule(static)") for (long long q = 0; q < n; ++q) v[q] = x;
   }
   inline double &operator()(int i, int j, int k = 1) {
     return v[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (size_t)(k - 1))];
@@ -64,9 +84,12 @@ struct A3 {
 };
 struct I3 {
   int n1 = 0, n2 = 0, n3 = 0;
-  std::vector<int32_t> v;
+  std::vector<int32_t, DefaultInit<int32_t>> v;
   void init(int a, int b, int c = 1, int x = 0) {
-    n1 = a; n2 = b; n3 = c; v.assign((size_t)a * b * c, x);
+    n1 = a; n2 = b; n3 = c;
+    const long long n = (long long)a * b * c;
+    v.resize((size_t)n);
+    _Pragma("omp parallel for schedule(static)") for (long long q = 0; q < n; ++q) v[q] = x;
   }
   inline int32_t &operator()(int i, int j, int k = 1) {
     return v[(size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (size_t)(k - 1))];
@@ -77,6 +100,9 @@ struct I3 {
 };
 
 #define PAR _Pragma("omp parallel for schedule(static)")
+// level x row nests: one work item per (k, j), so 2-D fields (n3 = 1) split
+// over rows too
+#define PAR2 _Pragma("omp parallel for collapse(2) schedule(static)")
 
 /* ---------------------------------------------------------------- literals */
 /* A default-REAL literal: rounded once to REAL(4) (gfortran) or kept (r8). */
@@ -249,15 +275,15 @@ struct Model {
     ans.init(ni, nj, n3, dft);
     if (hga.n == hgb.n) { fprintf(stderr, "no need to interpolate\n"); abort(); }
     if (hga.ew == &hgb) {
-      PAR for (int k = 1; k <= n3; ++k)
+      PAR2 for (int k = 1; k <= n3; ++k)
         for (int j = 1; j <= nj; ++j)
           for (int i = 1; i <= nim; ++i) ans(i + hga.si, j, k) = 0.5 * (var(i, j, k) + var(i + 1, j, k));
     } else if (hga.ns == &hgb) {
-      PAR for (int k = 1; k <= n3; ++k)
+      PAR2 for (int k = 1; k <= n3; ++k)
         for (int j = 1; j <= njm; ++j)
           for (int i = 1; i <= ni; ++i) ans(i, j + hga.sj, k) = 0.5 * (var(i, j, k) + var(i, j + 1, k));
     } else if (hga.di == &hgb) {
-      PAR for (int k = 1; k <= n3; ++k)
+      PAR2 for (int k = 1; k <= n3; ++k)
         for (int j = 1; j <= njm; ++j)
           for (int i = 1; i <= nim; ++i)
             ans(i + hga.si, j + hga.sj, k) =
@@ -272,14 +298,14 @@ struct Model {
     if (gb.ew != &ga) { ter(tmp, var, ga, *gb.ew); t = &tmp; }
     const int n3 = var.n3;
     ans.init(ni, nj, n3, 0.0);
-    PAR for (int k = 1; k <= n3; ++k)
+    PAR2 for (int k = 1; k <= n3; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= nim; ++i) {
           double d = (*t)(i + 1, j, k) - (*t)(i, j, k);
           if (mask) d = d * (*mask)(i + 1, j, k) * (*mask)(i, j, k);
           ans(i + ga.si, j, k) = d;
         }
-    PAR for (int k = 1; k <= n3; ++k)
+    PAR2 for (int k = 1; k <= n3; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = ans(i, j, k) / gb.dx1(i, j);
     swp(ans);
@@ -291,14 +317,14 @@ struct Model {
     if (gb.ns != &ga) { ter(tmp, var, ga, *gb.ns); t = &tmp; }
     const int n3 = var.n3;
     ans.init(ni, nj, n3, 0.0);
-    PAR for (int k = 1; k <= n3; ++k)
+    PAR2 for (int k = 1; k <= n3; ++k)
       for (int j = 1; j <= njm; ++j)
         for (int i = 1; i <= ni; ++i) {
           double d = (*t)(i, j + 1, k) - (*t)(i, j, k);
           if (mask) d = d * (*mask)(i, j + 1, k) * (*mask)(i, j, k);
           ans(i, j + ga.sj, k) = d;
         }
-    PAR for (int k = 1; k <= n3; ++k)
+    PAR2 for (int k = 1; k <= n3; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = ans(i, j, k) / gb.dx2(i, j);
     swp(ans);
@@ -306,7 +332,7 @@ struct Model {
   /* px_r3d_center, mod_op.f90:529-559 (hg = guj) */
   void px_center(A3 &ans, const A3 &var, const HG &hg) const {
     ans.init(ni, nj, var.n3, 0.0);
-    PAR for (int k = 1; k <= var.n3; ++k)
+    PAR2 for (int k = 1; k <= var.n3; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 2; i <= ni - 1; ++i) {
           double dx = C.a * hg.ew->rh(i, j) * (hg.ew->dx1(i, j) + hg.ew->dx1(i + 1, j));
@@ -317,14 +343,14 @@ struct Model {
   /* p3_r3d, mod_op.f90:715-735: var on gi1 (nkp) -> gi2 (nk) */
   void p3(A3 &ans, const A3 &var) const {
     ans.init(ni, nj, nk, 0.0);
-    PAR for (int k = 1; k <= nk; ++k)
+    PAR2 for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = (var(i, j, k) - var(i, j, k + 1)) / gi2.dpr[k];
   }
   /* pz_r3d, mod_op.f90:762-790: gi2 (nk) -> gi1 (nkp) */
   void pz(A3 &ans, const A3 &var, const I3 &msk) const {
     ans.init(ni, nj, nkp, 0.0);
-    PAR for (int k = 2; k <= nk; ++k)
+    PAR2 for (int k = 2; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           ans(i, j, k) = (var(i, j, k - 1) - var(i, j, k)) * msk(i, j, k - 1) * msk(i, j, k) / gi1.dz[k];
@@ -332,7 +358,7 @@ struct Model {
   /* dx3_r3d_b, mod_op.f90:792-811 */
   void dx3(A3 &ans, const A3 &var) const {
     ans.init(ni, nj, nkp, 0.0);
-    PAR for (int k = 2; k <= nk; ++k)
+    PAR2 for (int k = 2; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = var(i, j, k - 1) - var(i, j, k);
   }
@@ -340,12 +366,12 @@ struct Model {
   void vter(A3 &ans, const A3 &var, bool from_gi2) const {
     if (from_gi2) {
       ans.init(ni, nj, nkp, 0.0);
-      PAR for (int k = 2; k <= nk; ++k)
+      PAR2 for (int k = 2; k <= nk; ++k)
         for (int j = 1; j <= nj; ++j)
           for (int i = 1; i <= ni; ++i) ans(i, j, k) = (var(i, j, k - 1) + var(i, j, k)) * 0.5;
     } else {
       ans.init(ni, nj, nk, 0.0);
-      PAR for (int k = 1; k <= nk; ++k)
+      PAR2 for (int k = 1; k <= nk; ++k)
         for (int j = 1; j <= nj; ++j)
           for (int i = 1; i <= ni; ++i) ans(i, j, k) = (var(i, j, k) + var(i, j, k + 1)) * 0.5;
     }
@@ -370,7 +396,7 @@ struct Model {
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ax(i, j, k) = ax(i, j, k) / (C.a * gb.rh(i, j));
     p2(ay, var, ga, gc);
-    for (size_t q = 0; q < ay.v.size(); ++q) ay.v[q] = ay.v[q] / C.a;
+    PAR for (long long q = 0; q < (long long)ay.v.size(); ++q) ay.v[q] = ay.v[q] / C.a;
   }
   /* op_lap, mod_op.f90:904-925 */
   void lap(A3 &ans, const A3 &var, const HG &ga, const HG &gb) const {
@@ -453,14 +479,14 @@ struct Model {
   /* ---------------------------------------------------------- mod_den */
   /* den_alpha, mod_den.f90:33-55 */
   void den_alpha(A3 &alpha_, const A3 &t, const A3 &s, const A3 &ch) const {
-    PAR for (int k = 1; k <= nk; ++k)
+    PAR2 for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           if (g12.msk(i, j, k) == 1) alpha_(i, j, k) = 1.0 / den_rho(t(i, j, k), s(i, j, k), ch(i, j) * gi2.pr[k], r8);
   }
   /* den_prho, mod_den.f90:120-153 */
   void den_prho() {
-    PAR for (int k = 1; k <= nk; ++k)
+    PAR2 for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           if (g12.msk(i, j, k) > 0) {
@@ -508,7 +534,7 @@ struct Model {
         }
     div(wk3d, va, vb, g3j, g3j, g1j); /* wm%g%hg = g11%hg = g1j */
     vint(wk2d, wk3d, g12);
-    for (auto &x : wk2d.v) x = -x;
+    PAR for (long long q = 0; q < (long long)wk2d.v.size(); ++q) { double &x = wk2d.v[q]; x = -x; }
     for (int k = 2; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
@@ -535,7 +561,7 @@ struct Model {
     A3 wa, wb;
     ter(wa, var, g3j, *g3j.ew);
     ter(wb, var, g3j, *g3j.ns);
-    for (size_t q = 0; q < wa.v.size(); ++q) { wkm1.v[q] = wa.v[q] * u.v[q]; wkm2.v[q] = wb.v[q] * v.v[q]; }
+    PAR for (long long q = 0; q < (long long)wa.v.size(); ++q) { wkm1.v[q] = wa.v[q] * u.v[q]; wkm2.v[q] = wb.v[q] * v.v[q]; }
     p1(wa, wkm1, *g3j.ew, g3j);
     p2(wb, wkm2, *g3j.ns, g3j);
     ans.init(ni, nj, nk);
@@ -543,12 +569,12 @@ struct Model {
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = (wa(i, j, k) + wb(i, j, k)) / (C.a * g3j.rh(i, j));
     vter(wkap, var, true);
-    for (size_t q = 0; q < wkap.v.size(); ++q) wkap.v[q] = wkap.v[q] * w.v[q];
+    PAR for (long long q = 0; q < (long long)wkap.v.size(); ++q) wkap.v[q] = wkap.v[q] * w.v[q];
     for (int k = 2; k <= nkp - 1; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) wkbp(i, j, k) = wkap(i, j, k) * g32.msk(i, j, k - 1) * g32.msk(i, j, k);
     p3(wa, wkbp);
-    for (size_t q = 0; q < ans.v.size(); ++q) ans.v[q] = ans.v[q] + wa.v[q];
+    PAR for (long long q = 0; q < (long long)ans.v.size(); ++q) ans.v[q] = ans.v[q] + wa.v[q];
     p1(wkm1, u, *g3j.ew, g3j);
     p2(wkm2, v, *g3j.ns, g3j);
     p3(wa, w);
@@ -669,27 +695,27 @@ struct Model {
     for (int nt = 1; nt <= nstep; ++nt) {
       sch.fill(1.0);
       ter(wk, chp, g1j, g3j);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           if (g32.lev(i, j) > 0) sch(i, j) = std::sqrt(wk(i, j));
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           s1(i, j) = g32.prh(i, j) * sch(i, j) * ubp(i, j);
           s2(i, j) = g32.prh(i, j) * sch(i, j) * vbp(i, j);
         }
       div(wk, s1, s2, g3j, g3j, g1j);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           double w = chp(i, j) - wk(i, j) * bt * C.gamma_b / g12.prh(i, j);
           if (g12.lev(i, j) > 0) chc(i, j) = w;
         }
       ter(wk, chc, g1j, g3j);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           if (g32.lev(i, j) > 0) sch(i, j) = std::sqrt(wk(i, j));
       lap(l1, ubp, g3j, g3j);
       lap(l2, vbp, g3j, g3j);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           int seau = g32.msk(i, j, 1);
           vs1(i, j) = seau * am(i, j, 1) * l1(i, j);
@@ -698,30 +724,30 @@ struct Model {
       if (nt == 1) { v01 = vs1; v02 = vs2; }
       gra(gx, gy, chc, g1j, *g1j.ew, *g1j.ns);
       gi1_.fill(0.0); /* row nj never written by the reference (see header) */
-      for (int j = 1; j <= njm; ++j)
+      PAR for (int j = 1; j <= njm; ++j)
         for (int i = 1; i <= ni; ++i)
           gi1_(i, j) = 0.5 * (gx(i, j) * bphi_xn(i, j) + gx(i, j + 1) * bphi_xs(i, j + 1));
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= nim; ++i)
           gi2_(i, j) = 0.5 * (gy(i, j) * bphi_ye(i, j) + gy(i + 1, j) * bphi_yw(i + 1, j));
       swp(gi1_); swp(gi2_);
       ter(wk, chc, g1j, *g1j.ew);
       cg1.fill(0.0);
-      for (int j = 1; j <= njm; ++j)
+      PAR for (int j = 1; j <= njm; ++j)
         for (int i = 1; i <= ni; ++i)
           cg1(i, j) = 0.5 * (wk(i, j) * bgra_xn(i, j) + wk(i, j + 1) * bgra_xs(i, j + 1));
       ter(wk, chc, g1j, *g1j.ns);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= nim; ++i)
           cg2(i, j) = 0.5 * (wk(i, j) * bgra_ye(i, j) + wk(i + 1, j) * bgra_yw(i + 1, j));
       swp(cg1); swp(cg2);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           int seau = g32.msk(i, j, 1);
           pg1(i, j) = (gi1_(i, j) + cg1(i, j) + graphihx(i, j)) * seau * sch(i, j);
           pg2(i, j) = (gi2_(i, j) + cg2(i, j) + graphihy(i, j)) * seau * sch(i, j);
         }
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           int seau = g32.msk(i, j, 1);
           double p1_ = seau * (vs1(i, j) - v01(i, j) + ut(i, j) - pg1(i, j) + 0.5 * cor(i, j) * vbp(i, j));
@@ -739,24 +765,25 @@ struct Model {
           vbc(i, j) = p2_ * bt + vbp(i, j);
         }
       ubp = ubc; vbp = vbc;
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
           s1(i, j) = g32.prh(i, j) * sch(i, j) * ubc(i, j);
           s2(i, j) = g32.prh(i, j) * sch(i, j) * vbc(i, j);
         }
       div(wk, s1, s2, g3j, g3j, g1j);
-      for (int j = 1; j <= nj; ++j)
+      PAR for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) chc(i, j) = chp(i, j) - g12.msk(i, j, 1) * wk(i, j) * bt / g12.prh(i, j);
-      if (nt <= nstep / 2)
-        for (size_t q = 0; q < mch.v.size(); ++q) mch.v[q] = mch.v[q] + chc.v[q];
+      if (nt <= nstep / 2) {
+        PAR for (long long q = 0; q < (long long)mch.v.size(); ++q) mch.v[q] = mch.v[q] + chc.v[q];
+      }
       chp = chc;
-      for (size_t q = 0; q < ua.v.size(); ++q) {
+      PAR for (long long q = 0; q < (long long)ua.v.size(); ++q) {
         ua.v[q] = ua.v[q] + ubc.v[q];
         va.v[q] = va.v[q] + vbc.v[q];
         mch2.v[q] = mch2.v[q] + chc.v[q];
       }
     }
-    for (size_t q = 0; q < ua.v.size(); ++q) {
+    PAR for (long long q = 0; q < (long long)ua.v.size(); ++q) {
       ubc.v[q] = ua.v[q] / (nstep + 1);
       vbc.v[q] = va.v[q] / (nstep + 1);
       ubp.v[q] = ubc.v[q];
@@ -772,7 +799,7 @@ struct Model {
 
   /* smag, mod_int.f90:403-440 */
   void smag(const A3 &u, const A3 &v) {
-    PAR for (int k = 1; k <= nk; ++k)
+    PAR2 for (int k = 1; k <= nk; ++k)
       for (int j = 2; j <= nj - 1; ++j)
         for (int i = 2; i <= ni - 1; ++i) {
           double dx = C.a * (g4j.rh(i, j) * g4j.dx1(i, j) + g4j.rh(i + 1, j) * g4j.dx1(i + 1, j));
@@ -855,7 +882,7 @@ struct Model {
           uu(i, j, k) = uc(i, j, k) * sch(i, j) / mch2(i, j);
           vv(i, j, k) = vc(i, j, k) * sch(i, j) / mch2(i, j);
         }
-    for (size_t q = 0; q < uu.v.size(); ++q) {
+    PAR for (long long q = 0; q < (long long)uu.v.size(); ++q) {
       acu.v[q] = acu.v[q] + uu.v[q];
       acv.v[q] = acv.v[q] + vv.v[q];
     }
@@ -881,7 +908,7 @@ struct Model {
   void op_adv_ts(A3 &ans, const A3 &var) {
     A3 sch, u1(ni, nj, nk), u2(ni, nj, nk), w1, w2, wa, wb, tmp(ni, nj, nk), wkp, wmp(ni, nj, nkp);
     ter(sch, chc, g1j, g3j, 1.0);
-    for (auto &x : sch.v) x = std::sqrt(x);
+    PAR for (long long q = 0; q < (long long)sch.v.size(); ++q) { double &x = sch.v[q]; x = std::sqrt(x); }
     for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) {
@@ -891,20 +918,20 @@ struct Model {
     p1(w1, var, g1j, *g1j.ew);
     p2(w2, var, g1j, *g1j.ns);
     ter(wa, u1, g3j, *g1j.ew);
-    for (size_t q = 0; q < tmp.v.size(); ++q) tmp.v[q] = wa.v[q] * w1.v[q];
+    PAR for (long long q = 0; q < (long long)tmp.v.size(); ++q) tmp.v[q] = wa.v[q] * w1.v[q];
     ter(wb, tmp, *g1j.ew, g1j);
     ans.init(ni, nj, nk);
     for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = wb(i, j, k) / (C.a * g1j.rh(i, j));
     ter(wa, u2, g3j, *g1j.ns);
-    for (size_t q = 0; q < tmp.v.size(); ++q) tmp.v[q] = wa.v[q] * w2.v[q];
+    PAR for (long long q = 0; q < (long long)tmp.v.size(); ++q) tmp.v[q] = wa.v[q] * w2.v[q];
     ter(wb, tmp, *g1j.ns, g1j);
     for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) ans(i, j, k) = ans(i, j, k) + wb(i, j, k) / (C.a * g1j.rh(i, j));
     dx3(wkp, var);
-    for (size_t q = 0; q < wmp.v.size(); ++q) wmp.v[q] = wm.v[q] * wkp.v[q];
+    PAR for (long long q = 0; q < (long long)wmp.v.size(); ++q) wmp.v[q] = wm.v[q] * wkp.v[q];
     vter(wa, wmp, false);
     for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
@@ -919,7 +946,7 @@ struct Model {
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) w1(i, j, k) = w1(i, j, k) / (C.a * g2j.rh(i, j));
     p2(w2, var, g1j, *g1j.ns, &g12.msk);
-    for (auto &x : w2.v) x = x / C.a;
+    PAR for (long long q = 0; q < (long long)w2.v.size(); ++q) { double &x = w2.v[q]; x = x / C.a; }
     ter(c1, ch, g1j, *g1j.ew);
     ter(c2, ch, g1j, *g1j.ns);
     for (int k = 1; k <= nk; ++k)
@@ -930,13 +957,13 @@ struct Model {
         }
     div(wk, va, vb, *g1j.ew, *g1j.ns, g1j);
     ans.init(ni, nj, nk);
-    for (size_t q = 0; q < wk.v.size(); ++q) ans.v[q] = C.ah_c * wk.v[q];
+    PAR for (long long q = 0; q < (long long)wk.v.size(); ++q) ans.v[q] = C.ah_c * wk.v[q];
     pz(wkp, var, g12.msk);
     for (int k = 1; k <= nkp; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) wkp(i, j, k) = C.g * C.rho0 * kh(i, j, k) * wkp(i, j, k);
     p3(wk, wkp);
-    for (size_t q = 0; q < ans.v.size(); ++q) ans.v[q] = ans.v[q] + wk.v[q];
+    PAR for (long long q = 0; q < (long long)ans.v.size(); ++q) ans.v[q] = ans.v[q] + wk.v[q];
   }
 
   /* mix, mod_int.f90:583-600 */
@@ -1013,7 +1040,7 @@ struct Model {
     op_dif(d1, mch, tp);
     op_dif(d2, mch, sp);
     A3 p1_(ni, nj, nk), p2_(ni, nj, nk);
-    for (size_t q = 0; q < p1_.v.size(); ++q) {
+    PAR for (long long q = 0; q < (long long)p1_.v.size(); ++q) {
       p1_.v[q] = -a1.v[q];
       p2_.v[q] = -a2.v[q];
       p1_.v[q] = p1_.v[q] + d1.v[q];
@@ -1038,13 +1065,13 @@ struct Model {
           if (g12.msk(i, j, k) > 0 && tc(i, j, k) < C.tice) tc(i, j, k) = C.tice;
     convect();
     tp = tc; sp = sc;
-    for (size_t q = 0; q < act.v.size(); ++q) {
+    PAR for (long long q = 0; q < (long long)act.v.size(); ++q) {
       act.v[q] = act.v[q] + tc.v[q];
       acs.v[q] = acs.v[q] + sc.v[q];
     }
     /* den_alpha(wk, tp, sp, chc) then acr = acr + 1.0/wk; land points of the
      * reference's wk are never written: acr is left unchanged there. */
-    PAR for (int k = 1; k <= nk; ++k)
+    PAR2 for (int k = 1; k <= nk; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i)
           if (g12.msk(i, j, k) == 1) {
@@ -1174,9 +1201,9 @@ void Model::setup(const orc_inputs &in) {
           gkh(i, j, k) = in.vmix ? in.vmix[(size_t)(i - 1) + (size_t)glo_ni * ((j - 1) + (size_t)glo_nj * (k - 2))]
                                  : 9.96920996838687e+36;
     const double thr = r8 ? 9.0e+30 - 1.0 : (double)miss_thr;
-    for (auto &x : gkh.v) if (x > thr) x = L(0.1);
-    for (auto &x : gkh.v) if (x > L(200.0)) x = L(200.0);
-    for (auto &x : gkh.v) x = x * L(1.0e-4);
+    PAR for (long long q = 0; q < (long long)gkh.v.size(); ++q) { double &x = gkh.v[q]; if (x > thr) x = L(0.1); }
+    PAR for (long long q = 0; q < (long long)gkh.v.size(); ++q) { double &x = gkh.v[q]; if (x > L(200.0)) x = L(200.0); }
+    PAR for (long long q = 0; q < (long long)gkh.v.size(); ++q) { double &x = gkh.v[q]; x = x * L(1.0e-4); }
     for (int k = 1; k <= nkp; ++k)
       for (int j = 1; j <= nj; ++j)
         for (int i = 1; i <= ni; ++i) km(i, j, k) = C.km_c;
@@ -1352,7 +1379,7 @@ void Model::setup(const orc_inputs &in) {
       swp(*dst[q]);
     }
     const double miss = (double)(-9.99999e30f);
-    for (size_t q = 0; q < frc_taux.v.size(); ++q)
+    PAR for (long long q = 0; q < (long long)frc_taux.v.size(); ++q)
       if (frc_taux.v[q] == miss) {
         frc_taux.v[q] = 0.0; frc_tauy.v[q] = 0.0; frc_t.v[q] = 0.0;
         frc_s.v[q] = 0.0; frc_pa.v[q] = 0.0; frc_fw.v[q] = 0.0;
@@ -1414,6 +1441,11 @@ std::map<void *, std::map<std::string, VecView>> g_vec;
 extern "C" {
 
 void *orc_create(const orc_inputs *in) {
+  // the step allocates and frees whole-field temporaries (1-14 MB at 1
+  // degree) all the time: keep them on the heap and reuse the pages instead
+  // of mapping, faulting in and unmapping them on every call
+  mallopt(M_MMAP_THRESHOLD, 32 << 20);
+  mallopt(M_TRIM_THRESHOLD, 1 << 30);
   Model *m = new Model();
   m->setup(*in);
   return m;
