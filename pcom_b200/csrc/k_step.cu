@@ -625,7 +625,11 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ DevT<R>
   (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
+  // column-sum terms, the two column sums, and the new u, v of the first
+  // pass (as stored: rounded to R), which the second pass finishes without
+  // a round trip through global memory
   double *t1s = sh, *t2s = sh + nk * TB_X, *wsum = sh + 2 * nk * TB_X;
+  double *uns = wsum + 2 * TB_X, *vns = uns + nk * TB_X;
   int i, j;
   const bool ok = cell(P, i, j, true);
   const int tx = threadIdx.x;
@@ -690,8 +694,8 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ DevT<R>
     p2 = dvr(p2 * mu, w, rw);
     const double un = P.up[q] + p1 * bc;
     const double vn = P.vp[q] + p2 * bc;
-    P.uc[q] = un;  // in place; replaced below
-    P.vc[q] = vn;
+    uns[(k - 1) * TB_X + tx] = (double)(R)un;
+    vns[(k - 1) * TB_X + tx] = (double)(R)vn;
     t1s[(k - 1) * TB_X + tx] = un * P.dpr2[k] * mu;
     t2s[(k - 1) * TB_X + tx] = vn * P.dpr2[k] * mu;
   }
@@ -709,7 +713,7 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ DevT<R>
   const double schu = ld(P.schu, q2), mch2 = ld(P.mch2, q2), rmch2 = ld(P.rmch2, q2);
   for (int k = threadIdx.y + 1; k <= nk; k += TB_K) {
     const long long q = q2 + P.n2 * (k - 1);
-    double un = P.uc[q], vn = P.vc[q];
+    double un = uns[(k - 1) * TB_X + tx], vn = vns[(k - 1) * TB_X + tx];
     if (lu >= k) {
       un = un - w1 + ubc;
       vn = vn - w2 + vbc;
@@ -1242,6 +1246,8 @@ __global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ DevT<R
 static const dim3 kBlock3(TB_X, TB_K, 1);
 static inline dim3 g3(int nx, int ny, int nz) { return dim3((nx + TB_X - 1) / TB_X, ny, nz); }
 static inline size_t sm3(int nk, int planes) { return (size_t)planes * nk * TB_X * sizeof(double); }
+// k_clin: four level planes (column-sum terms, new u and v) and the two sums
+static inline size_t clin_smem(int nk) { return sm3(nk, 4) + 2 * TB_X * sizeof(double); }
 
 template <typename R>
 void launch_alpha_tobot(const DevT<R> &P, cudaStream_t s) { k_alpha_tobot<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
@@ -1264,7 +1270,11 @@ void launch_readyc3d(const DevT<R> &P, cudaStream_t s) {
 }
 template <typename R>
 void launch_clin(const DevT<R> &P, cudaStream_t s) {
-  k_clin<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2) + 2 * TB_X * sizeof(double), s>>>(P, nullptr);
+  const size_t smem = clin_smem(P.nk);
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(k_clin<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clin_smem(PCOM_MAXK));
+  (void)attr;
+  k_clin<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, smem, s>>>(P, nullptr);
 }
 template <typename R>
 void launch_smag(const DevT<R> &P, cudaStream_t s) {
@@ -1311,7 +1321,13 @@ void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cuda
   case BK_READYC3D:
     k_readyc_col<true><<<dim3((b.glo_ni + kRcX - 1) / kRcX, (b.nj + kRcY - 1) / kRcY, n), dim3(kRcX, kRcY), 0, s>>>(none, dPs);
     break;
-  case BK_CLIN: k_clin<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 2) + 2 * TB_X * sizeof(double), s>>>(none, dPs); break;
+  case BK_CLIN: {
+    static const cudaError_t attr = cudaFuncSetAttribute(k_clin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)clin_smem(PCOM_MAXK));
+    (void)attr;
+    k_clin<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, clin_smem(b.nk), s>>>(none, dPs);
+    break;
+  }
   case BK_SMAG: k_smag<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs); break;
   case BK_SSH: k_ssh<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
   case BK_TS:
