@@ -69,3 +69,19 @@ def test_calendar_and_daily_forcing(oracle_lib):
     o = oracle_lib.Oracle(c)
     o.step(25)  # crosses one day boundary at dtbc = 3600 s
     assert (o.const("year"), o.const("month"), o.const("day"), o.const("hour")) == (1, 1, 2, 1)
+
+
+def test_oracle_threads_bit_identical(oracle_lib):
+    # every parallel loop of the oracle is point-wise: one thread and four
+    # threads give the same bits for every field (across a day boundary)
+    c = make_case("tiny_bathy")
+    names = ("tc", "sc", "tp", "sp", "uc", "vc", "up", "vp", "chc", "chp", "ubc", "vbc", "alpha", "adp", "wm",
+             "am", "act", "acs", "acr", "acu", "acv", "acw", "mch", "mch2")
+    out = []
+    for threads in (1, 4):
+        o = oracle_lib.Oracle(c, threads=threads)
+        o.step(26)
+        out.append({f: o.field(f).copy() for f in names})
+        del o
+    for f in names:
+        assert out[0][f].tobytes() == out[1][f].tobytes(), f
