@@ -286,8 +286,9 @@ int pcom_gpu_batch_set_tiles(pcom_batch *b, int32_t tx, int32_t ty, int32_t max_
 int64_t pcom_gpu_batch_launch_count(pcom_batch *b);
 
 /* --- allocation-free barotropic subcycle -------------------------------- */
-/* No counterpart in the reference.  One int_trop subcycle (the same kernel
- * and arithmetic as pcom_gpu_step uses) over arrays the caller owns, for
+/* No counterpart in the reference.  One int_trop subcycle (the resident
+ * barotropic kernel: the arithmetic of pcom_gpu_step's int_trop, with IEEE
+ * divisions) over arrays the caller owns, for
  * callers that must not allocate device memory: code running while a stream
  * is being captured into a CUDA graph (cudaMalloc is not allowed there), and
  * host frameworks that hand every byte of device memory out from their own
