@@ -22,8 +22,15 @@
 #include "pcom_dev.cuh"
 #include "pcom_kernels.h"
 
+// block of the level-parallel 3-D kernels: 32 columns of one row x TB_K
+// threads down the levels.  8 (256 threads) rather than 16: the kernels
+// end in a serial column pass by one or two warps, and smaller blocks let
+// more of them per SM overlap that pass with other blocks' loads (1-degree
+// FP64 step 1.240 -> 1.188 ms).  k_pgra2d needs TB_K >= 8 (one column sum per
+// thread row).
 #define TB_X 32
-#define TB_K 16
+#define TB_K 8
+static_assert(TB_K >= 8, "k_pgra2d computes one of its 8 column sums per thread row");
 
 namespace {
 
