@@ -739,6 +739,7 @@ __global__ void __launch_bounds__(512, 2) k_clin(const __grid_constant__ DevT<R>
 
 // ----------------------------------------------------------------------------
 // smag (mod_int.f90:403-440): Smagorinsky viscosity, rows 2..nj-1.
+constexpr int kSmagK = 4;  // levels per thread of a single-domain launch
 template <typename R, bool BATCH>
 __global__ void k_smag(const __grid_constant__ DevT<R> P0, const DevT<R> *__restrict__ Ps) {
   const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
@@ -754,7 +755,11 @@ __global__ void k_smag(const __grid_constant__ DevT<R> P0, const DevT<R> *__rest
   const R dy = __ldg(P.dys1d + j - 1), rdy = __ldg(P.rdys1d + j - 1);
   const R tn = ld(P.tn3, q2);
   const R *u = P.uu, *v = P.vv;
-  for (int k = 1; k <= P.nk; ++k) {
+  // one domain: grid z splits the levels into groups of kSmagK; a batch
+  // (grid z = member) walks all levels
+  const int k0 = BATCH ? 1 : (int)blockIdx.z * kSmagK + 1;
+  const int k1 = BATCH ? P.nk : min(P.nk, k0 + kSmagK - 1);
+  for (int k = k0; k <= k1; ++k) {
   const long long q = q2 + P.n2 * (k - 1);
   const R dt = dvr(4 * (ld(u, q + 1) - ld(u, q - 1)), dx, rdx) - dvr(4 * (ld(v, q + ni) - ld(v, q - ni)), dy, rdy) +
                     DIVA(ld(v, q) * tn);
@@ -1285,7 +1290,9 @@ void launch_clin(const DevT<R> &P, cudaStream_t s) {
 }
 template <typename R>
 void launch_smag(const DevT<R> &P, cudaStream_t s) {
-  if (P.nj > 2) k_smag<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, 1), dim3(32, 4), 0, s>>>(P, nullptr);
+  if (P.nj > 2)
+    k_smag<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, (P.nk + kSmagK - 1) / kSmagK), dim3(32, 4), 0, s>>>(
+        P, nullptr);
 }
 template <typename R>
 void launch_ssh(const DevT<R> &P, cudaStream_t s) { k_ssh<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
