@@ -199,17 +199,23 @@ __global__ void k_uv2d(const __grid_constant__ DevT<R> P0, const DevT<R> *__rest
     st2(P.rsch2, P, i, q2, 1.0 / (s * s));
     st2(P.rchc, P, i, q2, 1.0 / P.chc[q2]);
     st2(P.sch_w, P, i, q2, sqrt(terTU(P, P.chp, i, j, 0.0)));
-  } else if (mode == 1) {
-    st2(P.sch_r, P, i, q2, sqrt(terTU(P, P.chc, i, j, 1.0)));
-    st2(P.sch_w, P, i, q2, sqrt(terTU(P, P.chp, i, j, 0.0)));
-    st2(P.rmch, P, i, q2, 1.0 / P.mch[q2]);
-    st2(P.rgm2, P, i, q2, 1.0 / (P.c.g * P.mch2[q2]));
   } else {
-    double s = 1.0;
-    if (P.lev_u[q2] > 0) s = sqrt(terTU(P, P.mch, i, j, 1.0));
-    st2(P.schc, P, i, q2, s);
-    st2(P.schu, P, i, q2, sqrt(terTU(P, P.mch2, i, j, 1.0)));
-    st2(P.rmch2, P, i, q2, 1.0 / P.mch2[q2]);
+    // mode 2: int_clin's fields; mode 1: int_ts's; mode 3: both (all read
+    // only the barotropic subcycle's chc, chp, mch, mch2, which nothing
+    // between int_clin and int_ts changes)
+    if (mode != 1) {
+      double s = 1.0;
+      if (P.lev_u[q2] > 0) s = sqrt(terTU(P, P.mch, i, j, 1.0));
+      st2(P.schc, P, i, q2, s);
+      st2(P.schu, P, i, q2, sqrt(terTU(P, P.mch2, i, j, 1.0)));
+      st2(P.rmch2, P, i, q2, 1.0 / P.mch2[q2]);
+    }
+    if (mode != 2) {
+      st2(P.sch_r, P, i, q2, sqrt(terTU(P, P.chc, i, j, 1.0)));
+      st2(P.sch_w, P, i, q2, sqrt(terTU(P, P.chp, i, j, 0.0)));
+      st2(P.rmch, P, i, q2, 1.0 / P.mch[q2]);
+      st2(P.rgm2, P, i, q2, 1.0 / (P.c.g * P.mch2[q2]));
+    }
   }
 }
 

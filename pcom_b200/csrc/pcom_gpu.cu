@@ -620,10 +620,12 @@ int do_trop(pcom_handle *h) {
   h->n_ch++;
   return PCOM_OK;
 }
-int do_clin_uv(pcom_handle *h) {
+// with_ts2d: the 2-D prep of int_ts (its sch, reciprocals of mch, mch2) in
+// the same launch as int_clin's (both read only int_trop's outputs)
+int do_clin_uv(pcom_handle *h, bool with_ts2d = false) {
   {
     Prof p(h, "clin_2d");
-    ON_DEV(launch_uv2d(X, 2, h->stream));
+    ON_DEV(launch_uv2d(X, with_ts2d ? 3 : 2, h->stream));
   }
   {
     Prof p(h, "int_clin");
@@ -644,8 +646,8 @@ int do_ssh(pcom_handle *h) {
   h->n_ssh++;
   return PCOM_OK;
 }
-int do_ts(pcom_handle *h) {
-  {
+int do_ts(pcom_handle *h, bool with_2d = true) {
+  if (with_2d) {
     Prof p(h, "ts_2d");
     ON_DEV(launch_uv2d(X, 1, h->stream));
   }
@@ -719,13 +721,13 @@ int enqueue_step(pcom_handle *h, int64_t iter) {
   CK(cudaStreamWaitEvent(h->stream, h->ev_join[0], 0));
   if ((rc = do_readyc_3d(h, iter))) return rc;
   if ((rc = do_trop(h))) return rc;
-  if ((rc = do_clin_uv(h))) return rc;
+  if ((rc = do_clin_uv(h, true))) return rc;
   CK(cudaEventRecord(h->ev_fork[1], h->stream));
   CK(cudaStreamWaitEvent(h->side, h->ev_fork[1], 0));
   if ((rc = do_smag(h, h->side))) return rc;
   CK(cudaEventRecord(h->ev_join[1], h->side));
   if ((rc = do_ssh(h))) return rc;
-  if ((rc = do_ts(h))) return rc;
+  if ((rc = do_ts(h, false))) return rc;
   CK(cudaStreamWaitEvent(h->stream, h->ev_join[1], 0));
   CK(cudaGetLastError());
   return PCOM_OK;

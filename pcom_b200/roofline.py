@@ -33,11 +33,11 @@ FIELDS = {
     "upwelling": (3, 4),                   # R uc, vc; W wm
     "readyc_3d": (2 + 1 + 2 + 4 + 1, 6),   # R uc, vc, wm, am, (km); W auc, avc, fx, fy
     "int_trop": (0, 30),                   # statics once; substeps below
-    "clin_2d": (0, 5),
+    "clin_2d": (0, 5 + 6),                # int_clin's 2-D prep and, in the full step, int_ts's (one launch)
     "int_clin": (12 + 7, 8),               # R adp, alpha, 6 AB3, fx, fy, uc, vc, up, vp; W uc, vc, up, vp, uu, vv, acu
     "smag": (3, 2),
     "int_ssh": (3, 3),
-    "ts_2d": (0, 4),
+    "ts_2d": (0, 4),                       # its own launch only when phases run one by one
     "upwelling+acw": (6, 4),
     "int_ts": (4 + 2 + 1 + 2 + 1 + 2 + 6, 6),  # R tc, sc, tp, sp, uc, vc, wm, kh, prho(2); W tn, sn; RW act, acs, acr
     "den_prho": (4, 1),
