@@ -51,9 +51,9 @@ namespace {
 #define DIVDP(x, k) dvr((x), P.dpr2[k], P.rdpr2[k])
 
 // column/row of this thread; interior: i in 2..ni-1, else i in 1..ni
-template <typename R>
+template <int BX = TB_X, typename R>
 __device__ __forceinline__ bool cell(const DevT<R> &P, int &i, int &j, bool interior) {
-  const int x = blockIdx.x * TB_X + threadIdx.x;
+  const int x = blockIdx.x * BX + threadIdx.x;
   j = blockIdx.y + 1;
   if (interior) {
     i = x + 2;
@@ -220,6 +220,11 @@ __global__ void k_uv2d(const __grid_constant__ DevT<R> P0, const DevT<R> *__rest
 }
 
 // ----------------------------------------------------------------------------
+// columns per block of k_upwelling: 16 on the FP64 path (its serial column
+// pass then overlaps better with other blocks' loads: 50 -> 44 us and 57 ->
+// 49 us at 1 degree), 32 on the mixed path (no gain there)
+template <typename R>
+__host__ __device__ constexpr int upw_cols() { return std::is_same<R, double>::value ? 16 : TB_X; }
 // upwelling (mod_int.f90:626-647): wk3d = div(sqrt(ter(chp)) * (uc, vc)),
 // wm(k) = (wm(k-1) + dpr(k-1) (wk3d(k-1) - vint(wk3d))) msk(k).
 // with_acw: also int_ts's acw accumulation (mod_int.f90:458-461).
@@ -230,9 +235,10 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ DevT<
   (void)MIXED;
   extern __shared__ double sh[];
   const int nk = P.nk;
-  double *wk = sh, *tm = sh + nk * TB_X, *wmv = sh + 2 * nk * TB_X;
+  constexpr int UX = upw_cols<R>();
+  double *wk = sh, *tm = sh + nk * UX, *wmv = sh + 2 * nk * UX;
   int i, j;
-  const bool ok = cell(P, i, j, true);
+  const bool ok = cell<UX>(P, i, j, true);
   const int tx = threadIdx.x;
   const long long q2 = ok ? I2(P, i, j) : 0;
   const int lev = ok ? P.lev_t[q2] : 0;
@@ -256,20 +262,20 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ DevT<
     }
     const R A = DIVX(tEc - tEw, 1, i);
     const R w = DIVARH(A + B, 1, j);
-    wk[(k - 1) * TB_X + tx] = w;
-    tm[(k - 1) * TB_X + tx] = w * P.dpr2[k] * (R)(k <= lev);
+    wk[(k - 1) * UX + tx] = w;
+    tm[(k - 1) * UX + tx] = w * P.dpr2[k] * (R)(k <= lev);
   }
   __syncthreads();
   if (ok && threadIdx.y == 0) {
     double s = 0.0;
-    for (int k = 1; k <= nk; ++k) s = s + tm[(k - 1) * TB_X + tx];
+    for (int k = 1; k <= nk; ++k) s = s + tm[(k - 1) * UX + tx];
     const double wk2d = -dvr(s, ld(P.prh_t, q2), ld(P.rprh_t, q2));
     double wprev = P.wm[q2];
     wmv[tx] = wprev;
     for (int k = 2; k <= nk; ++k) {
-      double w = wprev + P.dpr2[k - 1] * (wk2d + wk[(k - 2) * TB_X + tx]);
+      double w = wprev + P.dpr2[k - 1] * (wk2d + wk[(k - 2) * UX + tx]);
       w = w * (double)(k <= lev);
-      wmv[(k - 1) * TB_X + tx] = w;
+      wmv[(k - 1) * UX + tx] = w;
       wprev = w;
     }
   }
@@ -277,7 +283,7 @@ __global__ void __launch_bounds__(512) k_upwelling(const __grid_constant__ DevT<
   if (!ok) return;
   for (int k = threadIdx.y + 1; k <= nk; k += TB_K) {
     const long long q = q2 + P.n2 * (k - 1);
-    const double w = wmv[(k - 1) * TB_X + tx];
+    const double w = wmv[(k - 1) * UX + tx];
     if (k >= 2) st2(P.wm, P, i, q, w);
     if (with_acw) {
       const double gm = P.c.g * ld(P.mch2, q2);
@@ -1277,7 +1283,9 @@ void launch_uv2d(const DevT<R> &P, int mode, cudaStream_t s) {
 }
 template <typename R>
 void launch_upwelling(const DevT<R> &P, int with_acw, cudaStream_t s) {
-  k_upwelling<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 3), s>>>(P, nullptr, with_acw);
+  constexpr int UX = upw_cols<R>();
+  k_upwelling<R, false><<<dim3((P.glo_ni + UX - 1) / UX, P.nj, 1), dim3(UX, TB_K, 1),
+                          (size_t)3 * P.nk * UX * sizeof(double), s>>>(P, nullptr, with_acw);
 }
 template <typename R>
 void launch_readyc3d(const DevT<R> &P, cudaStream_t s) {
@@ -1337,7 +1345,12 @@ void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cuda
   case BK_ALPHA_TOBOT: k_alpha_tobot<double, true><<<g3(b.ni, b.nj, n), kBlock3, sm3(b.nk, 1), s>>>(none, dPs); break;
   case BK_PGRA2D: k_pgra2d<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 4), s>>>(none, dPs); break;
   case BK_UV2D: k_uv2d<double, true><<<dim3((b.glo_ni + 31) / 32, (b.nj + 3) / 4, n), dim3(32, 4), 0, s>>>(none, dPs, arg); break;
-  case BK_UPWELLING: k_upwelling<double, true><<<g3(b.glo_ni, b.nj, n), kBlock3, sm3(b.nk, 3), s>>>(none, dPs, arg); break;
+  case BK_UPWELLING: {
+    constexpr int UX = upw_cols<double>();
+    k_upwelling<double, true><<<dim3((b.glo_ni + UX - 1) / UX, b.nj, n), dim3(UX, TB_K, 1),
+                                (size_t)3 * b.nk * UX * sizeof(double), s>>>(none, dPs, arg);
+    break;
+  }
   case BK_READYC3D:
     k_readyc_col<true><<<dim3((b.glo_ni + kRcX - 1) / kRcX, (b.nj + kRcY - 1) / kRcY, n), dim3(kRcX, kRcY), 0, s>>>(none, dPs);
     break;
