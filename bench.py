@@ -37,8 +37,9 @@ STEP_SECONDS = 3600
 YEAR_STEPS = 365 * 86400 / STEP_SECONDS  # 8760 steps per model year
 
 
-def sypd(seconds_per_step: float) -> float:
-    return (86400.0 / seconds_per_step) / YEAR_STEPS
+def sypd(seconds_per_step: float, dtbc: float = STEP_SECONDS) -> float:
+    """Simulated years per wall-clock day for steps of dtbc model seconds."""
+    return (86400.0 / seconds_per_step) * dtbc / (365 * 86400.0)
 
 
 def max_over_ranks(t_ms: float, world: int, device: str) -> float:
@@ -59,16 +60,32 @@ def replica_sypd(ms_per_step: float, world: int) -> float:
     return world * sypd(ms_per_step / 1000.0)
 
 
+METRIC = "SYPD at 1deg x 30L (360x160x30 near-global), FP64 plain path"
+
+
+def workload_config(case: dict, world: int) -> dict:
+    """The workload both arms time (the GPU arm and --impl reference)."""
+    return {
+        "workload": "global1: 360x160x30 1-degree near-global ocean, dtbc 3600 s, dtbt 60 s "
+                    "(120 barotropic substeps per step), one baroclinic step per step",
+        "grid": [case["glo_ni"], case["glo_nj"], case["nk"]],
+        "parallelism": "replicas" if world > 1 else "single GPU",
+        "l2": "inputs larger than L2: ~0.9 GB of resident state vs 126 MB L2",
+    }
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=48)
     p.add_argument("--warmup", type=int, default=4)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--cpu-sample-steps", type=int, default=2)
+    p.add_argument("--cpu-sample-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     p.add_argument("--no-closure", action="store_true", help="skip the closure-network leg")
+    p.add_argument("--no-global025", action="store_true", help="skip the 0.25-degree leg")
+    p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     p.add_argument("--workload", default="global1", choices=["global1", "ensemble"],
                    help="ensemble: 32 perturbed 1-degree members + 16 uneven basins, batched")
     p.add_argument("--members", type=int, default=32)
@@ -299,6 +316,12 @@ def run_ours(args):
     closure = None
     if not args.no_closure:
         closure = run_closure_leg(args, case, ms_per_step)
+    # the 0.25-degree grid (bandwidth-sized) and the batched ensemble: N = 1 only
+    global025 = ensemble = None
+    if world == 1 and not args.no_global025:
+        global025 = run_global025_leg(args)
+    if world == 1 and not args.no_ensemble:
+        ensemble = ensemble_measure(args, steps=min(steps, 24), print_line=False)
 
     # ------------------------------------------------ CPU baseline (rank 0, N = 1)
     cpu = None
@@ -308,7 +331,7 @@ def run_ours(args):
     if rank == 0:
         clocks = clk.summary()
         line = {
-            "metric": "SYPD at 1deg x 30L (360x160x30 near-global), FP64 plain path",
+            "metric": METRIC,
             "value": round(value, 2),
             "unit": "SYPD",
             "n_gpus": world,
@@ -320,15 +343,9 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring)",
-            "config": {
-                "workload": "global1: 360x160x30 1-degree near-global ocean, dtbc 3600 s, dtbt 60 s "
-                            "(120 barotropic substeps per step), one baroclinic step per step",
-                "grid": [case["glo_ni"], case["glo_nj"], nk],
-                "parallelism": "replicas" if world > 1 else "single GPU",
-                "l2": "inputs larger than L2: ~0.9 GB of resident state vs 126 MB L2",
-                "timing": "CUDA events on the model's stream; kernels and roofline from a second timed pass "
-                          "of the same K steps with an event pair around every kernel",
-            },
+            "config": workload_config(case, world),
+            "timing": "CUDA events on the model's stream; kernels and roofline from a second timed pass "
+                      "of the same K steps with an event pair around every kernel",
             "ms_per_step_with_kernel_events": round(t_prof / steps, 4),
             "e2e": {"value": round(e2e, 2), "unit": "SYPD", "h2d_bytes_per_step": 5 * n2 * 8,
                     "d2h_bytes_per_step": 3 * n2 * 8,
@@ -345,6 +362,8 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "mixed": mixed,
             "closure": closure,
+            "global025": global025,
+            "ensemble": ensemble,
         }
         print(json.dumps(line))
     m.close()
@@ -473,6 +492,27 @@ def run_closure_leg(args, case, plain_ms):
             "note": "cost of the closure form on this grid with random weights; accuracy: pcom_b200.closure"}
 
 
+def run_global025_leg(args, steps: int = 8):
+    """The 1440x640x30 0.25-degree case (dtbc 1200 s, dtbt 20 s), FP64 and
+    mixed: time per step (CUDA events, device-resident, ~10 GB of state) and
+    the per-kernel algorithmic GB/s of a second pass with kernel events."""
+    from pcom_b200.roofline import kernel_table
+    from pcom_b200.synth import make_case
+
+    case = make_case("global025")
+    out = {"grid": [case["glo_ni"], case["glo_nj"], case["nk"]], "dtbc": case["dtbc"], "dtbt": case["dtbt"],
+           "steps": steps}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        t = kernel_table(case, mixed, steps)
+        ms = t["ms_per_step"]
+        top = dict(list(t["kernels"].items())[:6])
+        out[name] = {"ms_per_step": ms, "value": round(sypd(ms / 1000.0, case["dtbc"]), 2), "unit": "SYPD",
+                     "kernels": {k: {"us": v["us_per_launch"], "GB_s": v["GB_s"], "frac": v["frac_of_peak"]}
+                                 for k, v in top.items()},
+                     "peak_GB_s": t["peak_GB_s"], "peak_source": t["peak_source"]}
+    return out
+
+
 def ensemble_cases(members: int, basins: int, member_case: str = "box"):
     """Members of one case (default the 128x64x20 1-degree box) with seeded
     N(0, 0.05 K) perturbations of T (seeds 1..members), and idealized basins
@@ -490,6 +530,10 @@ def ensemble_cases(members: int, basins: int, member_case: str = "box"):
 
 
 def run_ensemble(args):
+    ensemble_measure(args, args.steps, print_line=True)
+
+
+def ensemble_measure(args, steps: int, print_line: bool):
     """Aggregate SYPD of a batched ensemble vs the same members stepped one
     after another through the single-domain path (same stream, same models)."""
     import ctypes as C
@@ -517,7 +561,6 @@ def run_ensemble(args):
     b.run(3)  # capture the graph of every ring phase
     it0 = models[0].iter
     day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
-    steps = args.steps
 
     def timed(body):
         torch.cuda.synchronize()
@@ -630,10 +673,13 @@ def run_ensemble(args):
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "cpu_baseline": None,
     }
-    print(json.dumps(line))
     b.close()
     for m in models:
         m.close()
+    if print_line:
+        print(json.dumps(line))
+    return {k: line[k] for k in ("metric", "value", "unit", "steps", "ms_per_step", "config", "sequential", "e2e",
+                                 "gpu_launches", "clocks")}
 
 
 def cpu_baseline(nsteps: int):
@@ -653,6 +699,9 @@ def cpu_baseline(nsteps: int):
 
 
 def run_reference(args):
+    """The reference algorithm's CPU implementation (the oracle's C++
+    restatement, OpenMP over all host threads) on the GPU arm's workload,
+    --warmup and --steps: rank 0 only."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -661,26 +710,26 @@ def run_reference(args):
     from pcom_b200.synth import make_case
 
     threads = os.cpu_count() or 1
-    o = pyoracle.Oracle(make_case(CASE), threads=threads)
-    warm = max(1, min(args.warmup, 2))
+    case = make_case(CASE)
+    o = pyoracle.Oracle(case, threads=threads)
+    warm = max(args.warmup, 3)
     o.step(warm)
-    # each timed step is one full baroclinic step; the sample is bounded so the
-    # run ends within minutes even for large --steps
-    nsteps = max(1, min(args.steps, 4))
+    # ~0.5 s per step on a 16-core host: the default 48 steps take ~25 s
+    nsteps = args.steps
     t0 = time.perf_counter()
     o.step(nsteps)
     dt = (time.perf_counter() - t0) / nsteps
     v = sypd(dt)
     line = {
         "impl": "reference",
-        "metric": "SYPD at 1deg x 30L (360x160x30 near-global), FP64 plain path",
+        "metric": METRIC,
         "value": round(v, 3), "unit": "SYPD", "n_gpus": world, "steps": nsteps, "warmup": warm,
         "ms_per_step": round(dt * 1000, 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring)",
-        "config": {"workload": "global1: 360x160x30 1-degree near-global ocean, dtbc 3600 s, dtbt 60 s",
-                   "grid": [360, 160, 30], "parallelism": "host threads"},
+        "config": workload_config(case, world),
+        "timing": f"wall clock around {nsteps} steps of the CPU restatement on {threads} host threads",
         "cpu_baseline": {"value": round(v, 3), "unit": "SYPD", "cores": threads, "kind": "port",
-                         "sample": f"{nsteps} steps after {warm} warm-up steps"},
+                         "sample": f"{nsteps} steps of the 360x160x30 case after {warm} warm-up steps"},
         "e2e": {"value": round(v, 3), "unit": "SYPD", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

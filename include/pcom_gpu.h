@@ -7,8 +7,8 @@
  * int_clin, int_ssh, int_ts) plus the daily den_prho (main.f90:179,200),
  * operating on module-global arrays (mod_arrays.f90:28-122).  This header is
  * the drop-in boundary for that block: a Fortran driver binds it with
- * ISO_C_BINDING and keeps its own setup, calendar, namelist
- * and netCDF I/O.
+ * ISO_C_BINDING (the interface module include/pcom_gpu.f90) and keeps its own
+ * setup, calendar, namelist and netCDF I/O.
  *
  * Conventions
  *  - Every array is a plain host pointer in Fortran order (i fastest) over the
@@ -288,19 +288,26 @@ int64_t pcom_gpu_batch_launch_count(pcom_batch *b);
 /* --- allocation-free barotropic subcycle -------------------------------- */
 /* No counterpart in the reference.  One int_trop subcycle (the resident
  * barotropic kernel: the arithmetic of pcom_gpu_step's int_trop, with IEEE
- * divisions) over arrays the caller owns, for
- * callers that must not allocate device memory: code running while a stream
- * is being captured into a CUDA graph (cudaMalloc is not allowed there), and
- * host frameworks that hand every byte of device memory out from their own
- * pool.  All pointers are device pointers in Fortran order; FP64 fields are
- * ni*nj (lev_* int32).  The metrics are given as separate components
- * (dxx = dx%x(1), dxy = dx%x(2)) of grids 1..4.  am1 is am(:,:,1).
+ * divisions) over arrays the caller owns, for callers that cannot let the
+ * library allocate device memory: host frameworks that own every byte of
+ * the GPU and hand it out from their own pool (a coupled-model driver that
+ * sizes one pool for all its components at start-up, a serving stack whose
+ * caching allocator holds the device), where a cudaMalloc inside the library
+ * would fail or break the framework's memory budget.  All pointers are device
+ * pointers in Fortran order; FP64 fields are ni*nj (lev_* int32).  The
+ * metrics are given as separate components (dxx = dx%x(1), dxy = dx%x(2)) of
+ * grids 1..4.  am1 is am(:,:,1).
  * The scratch this needs (halo ping-pong buffers, 1-D metric copies and the
- * grid-barrier words) is a fixed array inside the library, sized for
- * ni*nj <= PCOM_NOALLOC_MAX_POINTS and ni, nj <= PCOM_NOALLOC_MAX_DIM; larger
- * domains are rejected with PCOM_ERR_ARG.  The first call on a device looks
- * up that array's device address, so make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race. */
+ * grid-barrier words, about 3.2 MB) is a fixed array inside the library that
+ * every GPU which loads the library holds until the process exits; it is
+ * sized for ni*nj <= PCOM_NOALLOC_MAX_POINTS and ni, nj <= PCOM_NOALLOC_MAX_DIM
+ * (the 1-degree 362 x 162 domain fits); larger domains are rejected with
+ * PCOM_ERR_ARG.  The first call on a device (per CUDA context) looks up that
+ * array's device address, so make it before any stream capture.  The call
+ * clears the array's barrier and flag words itself; everything else in it is
+ * overwritten before use.  Calls share the array: calls that overlap on the
+ * GPU race.  The call waits on `stream` and returns once the subcycle has
+ * finished. */
 #define PCOM_NOALLOC_MAX_POINTS 65536
 #define PCOM_NOALLOC_MAX_DIM 1024
 typedef struct pcom_trop_io {

@@ -5,10 +5,11 @@
  * forcing (init/set_cf/calc_hpos/set_hgrid/set_vgrid/set_grid/calc_cf/inistat,
  * main.f90:252-704), then runs the time loop of main.f90:158-238 (daily
  * int_bnd + den_prho, then the per-step call block).  Its Fortran compiler is
- * not available in this build, so this C++ driver stands in for it: it does
+ * not available here, so this C++ driver stands in for it: it does
  * the same setup on the host, uploads the result through include/pcom_gpu.h
  * and drives the same loop.  A Fortran driver that keeps main.f90 calls
- * pcom_gpu.h directly instead.
+ * pcom_gpu.h directly instead, through the interface module
+ * include/pcom_gpu.f90.
  *
  * pcom_case mirrors what the reference reads from its input files for a
  * single-domain run: global interior arrays, Fortran order (i fastest).

@@ -11,6 +11,9 @@
 // central finite differences of the loss.  There is no reference counterpart
 // (the reference has no learned component); the layer definitions follow
 // include/pcom_cnn.h.
+#include <omp.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -45,6 +48,7 @@ long long tap_src(long long p, int t, int H, int W, int periodic_x) {
 
 // out[p][n] = sum_t sum_c in[src(p,t)][c] w[t][n][c] (FP64 accumulation)
 void conv_acc(int cin, int nout, const double *in, const double *w, long long npix, int H, int W, int px, double *out) {
+#pragma omp parallel for schedule(static)
   for (long long p = 0; p < npix; ++p)
     for (int n = 0; n < nout; ++n) {
       double s = 0.0;
@@ -75,18 +79,32 @@ void conv_back_data(int cin, int nout, const double *g, const double *w, long lo
     }
 }
 
+// pixels split into contiguous per-thread ranges, each summed into its own
+// buffer; the buffers are added in thread order (deterministic for a given
+// thread count)
 void conv_back_weight(int cin, int nout, const double *in, const double *g, long long npix, int H, int W, int px,
                       double *dw) {
-  for (long long p = 0; p < npix; ++p)
-    for (int t = 0; t < 9; ++t) {
-      const long long q = tap_src(p, t, H, W, px);
-      if (q < 0) continue;
-      for (int n = 0; n < nout; ++n) {
-        const double gv = g[p * nout + n];
-        double *d = dw + ((long long)t * nout + n) * cin;
-        for (int c = 0; c < cin; ++c) d[c] += in[q * cin + c] * gv;
+  const long long nw = 9LL * nout * cin;
+  const int nt = std::max(1, omp_get_max_threads());
+  std::vector<double> part((size_t)(nt * nw), 0.0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+    const long long p0 = npix * tid / nth, p1 = npix * (tid + 1) / nth;
+    double *acc = part.data() + (size_t)tid * nw;
+    for (long long p = p0; p < p1; ++p)
+      for (int t = 0; t < 9; ++t) {
+        const long long q = tap_src(p, t, H, W, px);
+        if (q < 0) continue;
+        for (int n = 0; n < nout; ++n) {
+          const double gv = g[p * nout + n];
+          double *d = acc + ((long long)t * nout + n) * cin;
+          for (int c = 0; c < cin; ++c) d[c] += in[q * cin + c] * gv;
+        }
       }
-    }
+  }
+  for (int t = 0; t < nt; ++t)
+    for (long long i = 0; i < nw; ++i) dw[i] += part[(size_t)t * nw + i];
 }
 
 constexpr int L = 5;

@@ -1,20 +1,25 @@
 // k_trop_noalloc.cu -- pcom_gpu_trop_noalloc: the barotropic subcycle for
 // callers that cannot allocate device memory.
 //
-// Who needs it: a caller that is capturing a stream into a CUDA graph may not
-// call cudaMalloc, and some host frameworks (coupled-model drivers, serving
-// stacks) own every byte of device memory and hand it out from their own
-// pool.  Such callers can own the inputs and outputs, but not the scratch the
-// subcycle needs.  This entry point keeps that scratch in one fixed array
-// compiled into the library (g_trop_scratch below, about 3.2 MB, held by every
-// GPU that loads the library until the process exits) and never allocates.
+// Who needs it: host frameworks that own every byte of device memory and
+// hand it out from their own pool -- a coupled-model driver that sizes its
+// pool for all components at start-up, or a serving stack whose caching
+// allocator already holds the GPU -- so a cudaMalloc from inside this library
+// would fail or break the framework's memory budget.  Such callers can own the
+// inputs and outputs, but not the scratch the subcycle needs.  This entry
+// point keeps that scratch in one fixed array compiled into the library
+// (g_trop_scratch below, about 3.2 MB, held by every GPU that loads the
+// library until the process exits) and never allocates.
 //
 // Limits: ni*nj <= PCOM_NOALLOC_MAX_POINTS and ni, nj <= PCOM_NOALLOC_MAX_DIM
 // (PCOM_NOALLOC_MAX_POINTS covers the 1-degree 362 x 162 domain); larger
 // domains are rejected.  Every call uses the same array, so two calls that
 // overlap on the GPU (different streams, or different host threads) race.
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress; make that first call before capturing a stream.
+// The first call on a device (in each CUDA context of that device) looks up
+// the array's device address with cudaGetSymbolAddress; make that first call
+// before any stream capture.  Each call waits on the caller's stream twice
+// (for the metric check and for the kernel's status words), so it returns
+// after the subcycle has finished on the GPU.
 #include <mutex>
 
 #include "../../include/pcom_gpu.h"
@@ -35,7 +40,28 @@ static __device__ __align__(256) double g_trop_scratch[kScratch];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
+// device address of g_trop_scratch per device, with the context it was looked
+// up in: a cudaDeviceReset destroys that context, the module is loaded again
+// in the next one and the array may move, so a new context means a new lookup
 double *g_addr[kMaxDevices] = {};
+void *g_ctx[kMaxDevices] = {};
+
+// the calling thread's current driver context (cuCtxGetCurrent through the
+// runtime's driver entry-point table; the library links no libcuda)
+typedef int (*ctx_get_fn)(void **);
+void *current_context() {
+  static ctx_get_fn fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (ctx_get_fn)f;
+  }();
+  void *ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 // 1-D copies of the j-only metrics and a check that dx%x(1) depends on i
 // only and dx%x(2), rh on j only (lat-lon grids, main.f90:408-493)
@@ -75,13 +101,17 @@ extern "C" int pcom_gpu_trop_noalloc(const pcom_trop_io *io, void *stream_) {
   double *base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    void *ctx = current_context();  // null before the runtime's first use of the device
+    if (!ctx || !g_addr[dev] || g_ctx[dev] != ctx) {
       // the host-side symbol is not a device address: look the address up
-      // once per device, with that device current
+      // once per device (and context), with that device current
       double *ptr = nullptr;
       cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_trop_scratch);
       if (e != cudaSuccess || !ptr) return error(PCOM_ERR_CUDA, "pcom_gpu_trop_noalloc: cudaGetSymbolAddress failed");
+      ctx = current_context();  // the lookup has initialised the context
+      if (!ctx) return error(PCOM_ERR_CUDA, "pcom_gpu_trop_noalloc: cannot read the current CUDA context");
       g_addr[dev] = ptr;
+      g_ctx[dev] = ctx;
     }
     base = g_addr[dev];
   }

@@ -16,6 +16,8 @@ Cases
               from a seeded Gaussian random field with a k^-2 power spectrum
               mapped to 0-5500 m (land where the field is negative), wind
               0.1 sin(3 lat), SST/SSS restoring.
+``global05``  720 x 320 x 30, the same generator at 0.5 deg with dtbt = 30 s,
+              dtbc = 1800 s (too many barotropic tiles for one per SM).
 ``global025`` 1440 x 640 x 30, the same generator at 0.25 deg with
               dtbt = 20 s, dtbc = 1200 s.
 ``basin``     glo_ni x glo_nj x nk (default 64 x 32 x 20) flat-bottom 1 deg
@@ -31,7 +33,7 @@ from __future__ import annotations
 
 import numpy as np
 
-CASES = ("tiny", "tiny_bathy", "box", "global1", "global025", "basin")
+CASES = ("tiny", "tiny_bathy", "box", "global1", "global05", "global025", "basin")
 
 
 def _grf(nx: int, ny: int, rng: np.random.Generator) -> np.ndarray:
@@ -86,6 +88,12 @@ def make_case(name: str = "box", seed: int = 1, noise: float = 0.01,
         bathy = True
         lat = -78.0 + np.arange(nj_, dtype=np.float64) * (158.0 / (nj_ - 1))
         lon = np.arange(ni_, dtype=np.float64) + 0.5
+    elif name == "global05":
+        ni_, nj_, nk_ = 720, 320, 30
+        bathy = True
+        lat = -78.0 + np.arange(nj_, dtype=np.float64) * (158.0 / (nj_ - 1))
+        lon = 0.5 * np.arange(ni_, dtype=np.float64) + 0.25
+        dtbt, dtbc = 30, 1800
     elif name == "global025":
         ni_, nj_, nk_ = 1440, 640, 30
         bathy = True

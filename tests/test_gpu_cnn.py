@@ -102,6 +102,63 @@ def test_wgrad(cin, nout, px):
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
 
 
+# the 1-degree closure's images: one 160 x 360 level image per model level,
+# periodic in x (the production strip walk of the persistent kernel)
+HF, WF, NF = 160, 360, 2
+
+
+@pytest.mark.parametrize("cin,nout,mode", [(16, 64, 0), (64, 64, 0), (64, 64, 2), (64, 16, 1), (64, 16, 2)])
+def test_conv_layer_full_shape(cin, nout, mode):
+    """Every convolution form the network uses, on two full 1-degree level
+    images (160 x 360, periodic in x), against the CPU restatement."""
+    import torch
+
+    rng = np.random.default_rng(100 + cin + nout + mode)
+    npix = HF * WF * NF
+    xd, x = bf16(rng.standard_normal((npix, cin)))
+    wd, w = bf16(rng.standard_normal((9, nout, cin)) / np.sqrt(9 * cin))
+    b = rng.standard_normal(nout).astype(np.float32)
+    bd = torch.from_numpy(b).cuda()
+    auxd, aux = bf16(rng.standard_normal((npix, nout)))
+    nstore = 4 if mode == 1 else 0
+    if mode == 1:
+        outd = torch.zeros((npix, nstore), dtype=torch.float32, device="cuda")
+    else:
+        outd = torch.zeros((npix, nout), dtype=torch.bfloat16, device="cuda")
+    rc = L.load().pcom_cnn_conv_layer(cin, nout, xd.data_ptr(), wd.data_ptr(), bd.data_ptr(),
+                                      auxd.data_ptr() if mode == 2 else None, outd.data_ptr(), npix, HF, WF, 1, mode,
+                                      nstore, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    cnn_check(rc, "conv")
+    torch.cuda.synchronize()
+    ref = pycnn.conv(cin, nout, x, w, b, aux if mode == 2 else None, HF, WF, 1, mode, nstore)
+    got = outd.float().cpu().numpy()
+    scale = np.abs(ref).max()
+    if mode == 1:
+        assert np.abs(got - ref).max() <= 1e-5 * scale
+    else:
+        assert np.abs(got - ref).max() <= 2 ** -8 * scale + 1e-6
+    # every pixel was written (the strip walk covers the whole image)
+    assert np.count_nonzero(np.abs(got - ref) > 2 ** -8 * scale + 1e-6) == 0
+
+
+@pytest.mark.parametrize("cin,nout", [(16, 64), (64, 64), (64, 16)])
+def test_wgrad_full_shape(cin, nout):
+    """The weight gradient over two full 1-degree level images."""
+    import torch
+
+    rng = np.random.default_rng(200 + cin + nout)
+    npix = HF * WF * NF
+    xd, x = bf16(rng.standard_normal((npix, cin)))
+    gd, g = bf16(rng.standard_normal((npix, nout)))
+    dw = torch.zeros(9 * nout * cin, dtype=torch.float32, device="cuda")
+    rc = L.load().pcom_cnn_wgrad_layer(cin, nout, xd.data_ptr(), gd.data_ptr(), dw.data_ptr(), npix, HF, WF, 1,
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    cnn_check(rc, "wgrad")
+    ref = pycnn.wgrad(cin, nout, x, g, HF, WF, 1)
+    got = dw.cpu().numpy().reshape(9, nout, cin)
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
 def _net(lib, nimg, H_, W_):
     h = C.c_void_p()
     cnn_check(lib.pcom_cnn_create(H_, W_, nimg, 1, C.byref(h)), "create")

@@ -35,8 +35,10 @@ def test_phase_by_phase(oracle_lib, name):
         o.phase("den_prho")
         m.set_forcing(m.int_bnd())
         m.den_prho()
-        r = compare(m.field("prho")[..., 0], o.field("prho1"))
-        assert r["unequal"] == 0
+        prho = m.field("prho")
+        for comp in (0, 1):  # prho%x(1) = d rho/dT, prho%x(2) = d rho/dS (mod_den.f90:143-150)
+            r = compare(prho[..., comp], o.field(f"prho{comp + 1}"))
+            assert r["unequal"] == 0, f"{name} step {it}: prho component {comp + 1} differs"
         for ph in PHASES:
             o.phase(ph)
             m.phase(ph, it)
@@ -59,6 +61,89 @@ def test_time_loop(oracle_lib, name, r8, steps):
     acc = m.accum()
     assert acc["n_ts"] == acc["n_uv"] == acc["n_ch"] == steps
     m.close()
+
+
+def test_config1_30_days(oracle_lib):
+    """The 128 x 64 x 20 box over 30 model days (720 steps of 3600 s, daily
+    int_bnd/den_prho, a month boundary): every state field and accumulator
+    bit-equal to the oracle."""
+    c = make_case("box")
+    o = oracle_lib.Oracle(c)
+    m = Model(c)
+    lev_t = m.static()["lev_t"]
+    m.run(720)
+    o.step(720)
+    assert m.iter == o.iter == 720
+    _check(m, o, STATE_FIELDS + ["acr"], lev_t, c["nk"], "box after 720 steps")
+    prho = m.field("prho")
+    for comp in (0, 1):
+        assert compare(prho[..., comp], o.field(f"prho{comp + 1}"))["unequal"] == 0
+    m.close()
+
+
+def _unstable_case(frac=0.05, k=2, seed=11):
+    """The box with T of levels k and k+1 (0-based) swapped in a seeded
+    fraction of its wet columns: colder water over warmer, so those columns
+    are statically unstable and convect (mod_int.f90:509-542) must mix them."""
+    c = make_case("box")
+    rng = np.random.default_rng(seed)
+    wet = c["itn"] >= k + 2
+    pick = wet & (rng.random(wet.shape) < frac)
+    pt = c["pt"].copy()
+    a, b = pt[k][pick], pt[k + 1][pick]
+    pt[k][pick], pt[k + 1][pick] = b, a
+    c["pt"] = pt
+    return c, pick
+
+
+def test_convective_adjustment(oracle_lib):
+    """Planted unstable columns: the oracle's int_ts mixes them (levels k and
+    k+1 end with equal T, which no stable column shows), and the CUDA path
+    gives the same fields bit for bit, phase by phase over 3 steps."""
+    k = 2
+    c, pick = _unstable_case(k=k)
+    assert pick.sum() > 100
+    o = oracle_lib.Oracle(c)
+    m = Model(c)
+    lev_t = m.static()["lev_t"]
+    for it in (1, 2, 3):
+        o.iter = it
+        o.phase("int_bnd")
+        o.phase("den_prho")
+        m.set_forcing(m.int_bnd())
+        m.den_prho()
+        for ph in PHASES:
+            o.phase(ph)
+            m.phase(ph, it)
+            _check(m, o, PHASE_FIELDS[ph], lev_t, c["nk"], f"unstable box step {it} {ph}")
+        if it == 1:
+            tc = o.field("tc")[:, 1:-1, 1:-1]
+            mixed = tc[k] == tc[k + 1]
+            assert mixed[pick].mean() > 0.9, "convect did not mix the planted columns"
+            assert mixed[~pick].mean() < 0.01
+        o.phase("advance")
+    m.close()
+
+
+def test_multi_tile_domain_picked_automatically(oracle_lib):
+    """720 x 320 x 30 (0.5 degree) has more barotropic tiles than the GPU
+    holds one per CTA: the automatic choice is the multi-tile kernel (forcing
+    the resident kernel is refused), and 2 steps are bit-equal to the oracle."""
+    from pcom_b200 import _lib as L
+
+    c = make_case("global05")
+    o = oracle_lib.Oracle(c)
+    m = Model(c)
+    lev_t = m.static()["lev_t"]
+    m.run(2)
+    o.step(2)
+    _check(m, o, STATE_FIELDS, lev_t, c["nk"], "global05 after 2 steps")
+    m.close()
+    r = Model(c)
+    L.check(r.lib.pcom_gpu_set_trop_kernel(r.handle, 1), "set_trop_kernel")
+    with pytest.raises(L.PcomError, match="does not fit the resident"):
+        r.run(1)
+    r.close()
 
 
 def test_full_size_one_step(oracle_lib):
