@@ -87,6 +87,10 @@ def parse():
     p.add_argument("--no-global025", action="store_true", help="skip the 0.25-degree leg")
     p.add_argument("--no-fma", action="store_true", help="skip the FMA-contracted legs")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    p.add_argument("--decomp", action="store_true",
+                   help="one 1-degree domain split into row slabs over the N ranks (strong scaling) "
+                        "instead of N replicas")
+    p.add_argument("--halo", type=int, default=2, help="halo rows of the row-slab split")
     p.add_argument("--workload", default="global1", choices=["global1", "ensemble"],
                    help="ensemble: 32 perturbed 1-degree members + 16 uneven basins, batched")
     p.add_argument("--members", type=int, default=32)
@@ -797,10 +801,71 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_decomp(args):
+    """One 1-degree domain split into row slabs, one per rank (pcom_b200.decomp:
+    3-D subroutines on each rank's rows, halo rows over NCCL after each, the
+    barotropic subcycle replicated from all-gathered 2-D inputs): SYPD of
+    that one domain, timed on the device as the max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from pcom_b200 import decomp as D
+    from pcom_b200.model import Model
+    from pcom_b200.synth import make_case
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    case = make_case(CASE)
+    m = Model(case)
+    slab = D.slabs(case["glo_nj"], world, args.halo)[rank]
+    e = D.GpuSlab(m, slab)
+    links = D.DistLinks(e, world) if world > 1 else D.LocalLinks({0: e})
+    drv = D.SlabDriver(links, args.halo)
+    drv.run(max(args.warmup, 3))
+    stream = e.stream
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = m.launch_count()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        drv.run(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
+    launches = m.launch_count() - launches0
+    m.check_finite()
+    ms = t / args.steps
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(sypd(ms / 1000.0), 2), "unit": "SYPD", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded k^-2 bathymetry, analytic wind and restoring)",
+            "config": dict(workload_config(case, 1), parallelism=f"row slabs over {world} ranks, halo {args.halo}"),
+            "slab_rows": [[s.lo, s.hi] for s in D.slabs(case["glo_nj"], world, args.halo)],
+            "gpu_launches": int(launches),
+            "clocks": {k: clk.summary()[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(line))
+    m.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.decomp:
+        run_decomp(a)
     elif a.workload == "ensemble":
         run_ensemble(a)
     else:

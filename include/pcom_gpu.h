@@ -175,6 +175,24 @@ int pcom_gpu_phase(pcom_handle *h, int32_t phase, int64_t tctr_i);
 int pcom_gpu_get_field(pcom_handle *h, const char *name, double *host, int64_t n);
 /* Element count of a named array (0 if unknown). */
 int64_t pcom_gpu_field_size(pcom_handle *h, const char *name);
+/* Device address of a named array (the current buffer: the AB3 history and
+ * the T/S pool rotate between steps, so ask again after each step), its
+ * element count and element size (8, or 4 for a 3-D field of a mixed
+ * handle).  For drivers that move parts of device arrays themselves, e.g.
+ * the halo rows of a domain split into row slabs.  No counterpart in the
+ * reference. */
+int pcom_gpu_field_ptr(pcom_handle *h, const char *name, void **dev, int64_t *count, int32_t *elem_bytes);
+/* Split the domain into row slabs (mod_param.f90:279-344 with npx = 1): the
+ * step's 3-D kernels and den_prho compute only rows j_lo..j_hi (padded
+ * 1-based index, within 1..nj; default 1..nj); the 2-D prep kernels and the
+ * barotropic subcycle still cover every row.  Every kernel keeps global row
+ * indexing, so a slab's rows come out exactly as in the whole-domain run
+ * once the driver has supplied the rows they read outside the slab (the
+ * halo rows of the 3-D fields and the other slabs' rows of the 2-D fields
+ * the barotropic subcycle reads; pcom_b200/decomp.py does this with
+ * torch.distributed).  Replaces the reference's y decomposition and its
+ * halo exchange (mod_mympi.f90:669-861). */
+int pcom_gpu_set_rows(pcom_handle *h, int32_t j_lo, int32_t j_hi);
 /* Run the NaN/Inf watchdog over the prognostic fields; PCOM_ERR_NUMERIC if
  * any wet point is not finite. */
 int pcom_gpu_check_finite(pcom_handle *h);

@@ -48,6 +48,15 @@ int pcom_model_destroy(pcom_model *m);
 pcom_handle *pcom_model_handle(pcom_model *m);
 /* n passes of the time loop body (main.f90:158-238, without output()). */
 int pcom_model_run(pcom_model *m, int64_t nsteps);
+/* One pass split open, for drivers that put their own work between the
+ * subroutines of the step (the halo exchanges of a domain split into row
+ * slabs): begin_step advances tctr%i (returned in *it) and on a new model
+ * day runs int_bnd and den_prho (main.f90:158-201; *new_day = 1); the caller
+ * then runs pcom_gpu_phase 0..6 with that counter and calls end_step, which
+ * advances the calendar (main.f90:231-232).  pcom_model_run is exactly
+ * begin_step, pcom_gpu_step, end_step. */
+int pcom_model_begin_step(pcom_model *m, int64_t *it, int32_t *new_day);
+int pcom_model_end_step(pcom_model *m);
 /* n passes of the time loop for n models stepped together through batch b
  * (pcom_gpu_batch_create on their handles, in the same order).  The models
  * must be at the same iteration and date (same bdate and dtbc): forcing

@@ -135,6 +135,15 @@ class Oracle:
             a = np.ctypeslib.as_array(ptr, shape=(n3.value, n2.value, n1.value)).copy()
         return a[0] if a.shape[0] == 1 and name not in ("z1", "pr1", "dz1", "dpr1", "z2", "pr2", "dz2", "dpr2", "lon", "lat") else a
 
+    def view(self, name: str) -> np.ndarray:
+        """The named array itself (writable, shares the oracle's memory),
+        numpy shape [n3][n2][n1]."""
+        n1, n2, n3 = C.c_int32(), C.c_int32(), C.c_int32()
+        ptr = lib().orc_field(self.h, name.encode(), C.byref(n1), C.byref(n2), C.byref(n3))
+        if not ptr:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(ptr, shape=(n3.value, n2.value, n1.value))
+
     def vec(self, name: str) -> np.ndarray:
         return self.field(name).reshape(-1)
 

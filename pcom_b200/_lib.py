@@ -99,6 +99,9 @@ SIGNATURES = {
     "pcom_gpu_phase": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
     "pcom_gpu_get_field": (C.c_int, [C.c_void_p, C.c_char_p, dbl_p, C.c_int64]),
     "pcom_gpu_field_size": (C.c_int64, [C.c_void_p, C.c_char_p]),
+    "pcom_gpu_field_ptr": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int32)]),
+    "pcom_gpu_set_rows": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "pcom_gpu_check_finite": (C.c_int, [C.c_void_p]),
     "pcom_gpu_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pcom_gpu_sync": (C.c_int, [C.c_void_p]),
@@ -152,6 +155,8 @@ SIGNATURES = {
     "pcom_model_destroy": (C.c_int, [C.c_void_p]),
     "pcom_model_handle": (C.c_void_p, [C.c_void_p]),
     "pcom_model_run": (C.c_int, [C.c_void_p, C.c_int64]),
+    "pcom_model_begin_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "pcom_model_end_step": (C.c_int, [C.c_void_p]),
     "pcom_model_run_batch": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_void_p, C.c_int64]),
     "pcom_model_iter": (C.c_int64, [C.c_void_p]),
     "pcom_model_date": (C.c_int, [C.c_void_p, i32_p]),

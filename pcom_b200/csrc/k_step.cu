@@ -57,14 +57,20 @@ namespace {
 template <int BX = TB_X, typename R>
 __device__ __forceinline__ bool cell(const DevT<R> &P, int &i, int &j, bool interior) {
   const int x = blockIdx.x * BX + threadIdx.x;
-  j = blockIdx.y + 1;
+  j = blockIdx.y + P.j_lo;
   if (interior) {
     i = x + 2;
-    return x < P.glo_ni && j <= P.nj;
+    return x < P.glo_ni && j <= P.j_hi;
   }
   i = x + 1;
-  return i <= P.ni && j <= P.nj;
+  return i <= P.ni && j <= P.j_hi;
 }
+
+// smag covers rows 2..nj-1 of the row window
+template <typename R>
+__host__ __device__ __forceinline__ int smag_j0(const DevT<R> &P) { return P.j_lo > 2 ? P.j_lo : 2; }
+template <typename R>
+__host__ __device__ __forceinline__ int smag_j1(const DevT<R> &P) { return P.j_hi < P.nj - 1 ? P.j_hi : P.nj - 1; }
 
 // ----------------------------------------------------------------------------
 // den_alpha (mod_den.f90:33-55) with T, S = tc, sc and ch = chc, fused with
@@ -476,8 +482,8 @@ __global__ void __launch_bounds__(kRcX * kRcY, 7) k_readyc_col(const __grid_cons
   using R = double;
   const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
   const int x = blockIdx.x * kRcX + threadIdx.x;
-  const int j = blockIdx.y * kRcY + threadIdx.y + 1;
-  if (x >= P.glo_ni || j > P.nj) return;
+  const int j = blockIdx.y * kRcY + threadIdx.y + P.j_lo;
+  if (x >= P.glo_ni || j > P.j_hi) return;
   const int i = x + 2;
   const int nk = P.nk;
   const long long n2 = P.n2;
@@ -761,8 +767,8 @@ __global__ void k_smag(const __grid_constant__ DevT<R> P0, const DevT<R> *__rest
   constexpr bool MIXED = std::is_same<R, float>::value;
   (void)MIXED;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  if (x >= P.glo_ni || j > P.nj - 1) return;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + smag_j0(P);
+  if (x >= P.glo_ni || j > smag_j1(P)) return;
   const int i = x + 2;
   const long long q2 = I2(P, i, j);
   const int ni = P.ni;
@@ -1066,8 +1072,8 @@ __global__ void __launch_bounds__(kColX * kColY, 7) k_ts_col(const __grid_consta
   using R = double;
   const DevT<R> &P = BATCH ? Ps[blockIdx.z] : P0;
   const int x = blockIdx.x * kColX + threadIdx.x;
-  const int j = blockIdx.y * kColY + threadIdx.y + 1;
-  if (x >= P.glo_ni || j > P.nj) return;
+  const int j = blockIdx.y * kColY + threadIdx.y + P.j_lo;
+  if (x >= P.glo_ni || j > P.j_hi) return;
   const int i = x + 2;
   const int nk = P.nk;
   const long long n2 = P.n2;
@@ -1272,14 +1278,17 @@ __global__ void __launch_bounds__(512) k_den_prho(const __grid_constant__ DevT<R
 // largest member and CTAs outside a smaller member's domain do nothing.
 static const dim3 kBlock3(TB_X, TB_K, 1);
 static inline dim3 g3(int nx, int ny, int nz) { return dim3((nx + TB_X - 1) / TB_X, ny, nz); }
+// rows of the handle's row window (all rows 1..nj unless the domain is split)
+template <typename R>
+static inline int wrows(const DevT<R> &P) { return P.j_hi - P.j_lo + 1; }
 static inline size_t sm3(int nk, int planes) { return (size_t)planes * nk * TB_X * sizeof(double); }
 // k_clin: four level planes (column-sum terms, new u and v) and the two sums
 static inline size_t clin_smem(int nk) { return sm3(nk, 4) + 2 * TB_X * sizeof(double); }
 
 template <typename R>
-void launch_alpha_tobot(const DevT<R> &P, cudaStream_t s) { k_alpha_tobot<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+void launch_alpha_tobot(const DevT<R> &P, cudaStream_t s) { k_alpha_tobot<R, false><<<g3(P.ni, wrows(P), 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
 template <typename R>
-void launch_pgra2d(const DevT<R> &P, cudaStream_t s) { k_pgra2d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
+void launch_pgra2d(const DevT<R> &P, cudaStream_t s) { k_pgra2d<R, false><<<g3(P.glo_ni, wrows(P), 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr); }
 template <typename R>
 void launch_uv2d(const DevT<R> &P, int mode, cudaStream_t s) {
   k_uv2d<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj + 3) / 4), dim3(32, 4), 0, s>>>(P, nullptr, mode);
@@ -1287,15 +1296,15 @@ void launch_uv2d(const DevT<R> &P, int mode, cudaStream_t s) {
 template <typename R>
 void launch_upwelling(const DevT<R> &P, int with_acw, cudaStream_t s) {
   constexpr int UX = upw_cols<R>();
-  k_upwelling<R, false><<<dim3((P.glo_ni + UX - 1) / UX, P.nj, 1), dim3(UX, TB_K, 1),
+  k_upwelling<R, false><<<dim3((P.glo_ni + UX - 1) / UX, wrows(P), 1), dim3(UX, TB_K, 1),
                           (size_t)3 * P.nk * UX * sizeof(double), s>>>(P, nullptr, with_acw);
 }
 template <typename R>
 void launch_readyc3d(const DevT<R> &P, cudaStream_t s) {
   if constexpr (std::is_same<R, double>::value)
-    k_readyc_col<false><<<dim3((P.glo_ni + kRcX - 1) / kRcX, (P.nj + kRcY - 1) / kRcY), dim3(kRcX, kRcY), 0, s>>>(P, nullptr);
+    k_readyc_col<false><<<dim3((P.glo_ni + kRcX - 1) / kRcX, (wrows(P) + kRcY - 1) / kRcY), dim3(kRcX, kRcY), 0, s>>>(P, nullptr);
   else
-    k_readyc3d<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr);
+    k_readyc3d<R, false><<<g3(P.glo_ni, wrows(P), 1), kBlock3, sm3(P.nk, 2), s>>>(P, nullptr);
 }
 template <typename R>
 void launch_clin(const DevT<R> &P, cudaStream_t s) {
@@ -1303,27 +1312,28 @@ void launch_clin(const DevT<R> &P, cudaStream_t s) {
   static const cudaError_t attr =
       cudaFuncSetAttribute(k_clin<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clin_smem(PCOM_MAXK));
   (void)attr;
-  k_clin<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, smem, s>>>(P, nullptr);
+  k_clin<R, false><<<g3(P.glo_ni, wrows(P), 1), kBlock3, smem, s>>>(P, nullptr);
 }
 template <typename R>
 void launch_smag(const DevT<R> &P, cudaStream_t s) {
-  if (P.nj > 2)
-    k_smag<R, false><<<dim3((P.glo_ni + 31) / 32, (P.nj - 2 + 3) / 4, (P.nk + kSmagK - 1) / kSmagK), dim3(32, 4), 0, s>>>(
+  const int rows = smag_j1(P) - smag_j0(P) + 1;
+  if (rows > 0)
+    k_smag<R, false><<<dim3((P.glo_ni + 31) / 32, (rows + 3) / 4, (P.nk + kSmagK - 1) / kSmagK), dim3(32, 4), 0, s>>>(
         P, nullptr);
 }
 template <typename R>
-void launch_ssh(const DevT<R> &P, cudaStream_t s) { k_ssh<R, false><<<g3(P.ni, P.nj, 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
+void launch_ssh(const DevT<R> &P, cudaStream_t s) { k_ssh<R, false><<<g3(P.ni, wrows(P), 1), kBlock3, sm3(P.nk, 1), s>>>(P, nullptr); }
 template <typename R>
 void launch_ts(const DevT<R> &P, cudaStream_t s) {
   if constexpr (std::is_same<R, double>::value) {
-    k_ts_col<false><<<dim3((P.glo_ni + kColX - 1) / kColX, (P.nj + kColY - 1) / kColY), dim3(kColX, kColY), 0, s>>>(P, nullptr);
-    k_ts_acc<false><<<g3(P.glo_ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr);
+    k_ts_col<false><<<dim3((P.glo_ni + kColX - 1) / kColX, (wrows(P) + kColY - 1) / kColY), dim3(kColX, kColY), 0, s>>>(P, nullptr);
+    k_ts_acc<false><<<g3(P.glo_ni, wrows(P), 1), kBlock3, 0, s>>>(P, nullptr);
   } else {
-    k_ts<R, false><<<g3(P.glo_ni, P.nj, 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr);
+    k_ts<R, false><<<g3(P.glo_ni, wrows(P), 1), kBlock3, sm3(P.nk, 4), s>>>(P, nullptr);
   }
 }
 template <typename R>
-void launch_den_prho(const DevT<R> &P, cudaStream_t s) { k_den_prho<R, false><<<g3(P.ni, P.nj, 1), kBlock3, 0, s>>>(P, nullptr); }
+void launch_den_prho(const DevT<R> &P, cudaStream_t s) { k_den_prho<R, false><<<g3(P.ni, wrows(P), 1), kBlock3, 0, s>>>(P, nullptr); }
 
 
 #define PCOM_INST(R)                                                   \

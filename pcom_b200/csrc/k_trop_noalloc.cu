@@ -129,6 +129,7 @@ extern "C" int pcom_gpu_trop_noalloc(const pcom_trop_io *io, void *stream_) {
 
   Dev D{};
   D.ni = ni; D.nj = nj; D.nim = ni - 1; D.njm = nj - 1; D.glo_ni = io->glo_ni; D.glo_nj = io->glo_nj;
+  D.j_lo = 1; D.j_hi = nj;
   D.bt = io->dtbt; D.bc = io->dtbc; D.nstep = io->dtbc / io->dtbt * 2;
   D.n2 = (long long)ni * nj;
   pcom_dev_consts((io->flags & PCOM_LIT_R8) != 0, D.c);

@@ -42,6 +42,11 @@ template <> struct Vec2<float> { using type = float2; };
 // state and scratch (always FP64).
 struct DevCommon {
   int ni, nj, nk, nkp, nim, njm, glo_ni, glo_nj;
+  // rows j_lo..j_hi (padded 1-based index) the step's 3-D kernels compute:
+  // 1..nj for a whole domain, this rank's slab of rows when the domain is
+  // split into row slabs across ranks (the 2-D prep kernels and the
+  // barotropic subcycle always cover every row)
+  int j_lo, j_hi;
   int bt, bc, nstep, rst;
   long long n2, n3, n3p;
   DevConsts c;

@@ -826,7 +826,7 @@ Named lookup(pcom_handle *h, const std::string &s) {
       {"acch", {D.acch, n2}}, {"acssh", {D.acssh, n2}}, {"cor", {D.cor, n2}},   {"cv1", {D.cv1, n2}},
       {"cv2", {D.cv2, n2}},   {"graphihx", {D.graphihx, n2}}, {"graphihy", {D.graphihy, n2}},
       {"sch_r", {D.sch_r, n2}}, {"sch_w", {D.sch_w, n2}}, {"bnd_taux", {D.taux, n2}}, {"bnd_tauy", {D.tauy, n2}},
-      {"bnd_t", {D.bnd_t, n2}}, {"bnd_s", {D.bnd_s, n2}}, {"bnd_pa", {D.bnd_pa, n2}}};
+      {"bnd_t", {D.bnd_t, n2}}, {"bnd_s", {D.bnd_s, n2}}, {"bnd_pa", {D.bnd_pa, n2}}, {"am1", {D.am1, n2}}};
   auto it2 = m2.find(s);
   if (it2 != m2.end()) return it2->second;
   // 3-D fields: FP64, or FP32 on the mixed path
@@ -1002,6 +1002,7 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   if (e != cudaSuccess) { pcom_gpu_destroy(h); return fail(PCOM_ERR_CUDA, "side stream: %s", cudaGetErrorString(e)); }
   Dev &D = h->D;
   D.ni = d.ni; D.nj = d.nj; D.nk = d.nk; D.nkp = d.nk + 1; D.nim = d.ni - 1; D.njm = d.nj - 1;
+  D.j_lo = 1; D.j_hi = d.nj;
   D.glo_ni = d.glo_ni; D.glo_nj = d.glo_nj;
   D.bt = d.dtbt; D.bc = d.dtbc; D.nstep = d.dtbc / d.dtbt * 2; D.rst = d.rst;
   D.n2 = h->n2; D.n3 = h->n3; D.n3p = h->n3p;
@@ -1456,6 +1457,27 @@ int pcom_gpu_get_field(pcom_handle *h, const char *name, double *host, int64_t n
   int rc = fetch(h, name, host);
   if (rc) return rc;
   return sync_check(h);
+}
+
+int pcom_gpu_set_rows(pcom_handle *h, int32_t j_lo, int32_t j_hi) {
+  if (!h) return fail(PCOM_ERR_ARG, "null handle");
+  if (j_lo < 1 || j_hi > h->nj || j_lo > j_hi)
+    return fail(PCOM_ERR_ARG, "rows %d..%d are not a range within 1..%d", j_lo, j_hi, h->nj);
+  CK(cudaStreamSynchronize(h->stream));
+  h->D.j_lo = j_lo;
+  h->D.j_hi = j_hi;
+  sync_common(h);
+  return PCOM_OK;
+}
+
+int pcom_gpu_field_ptr(pcom_handle *h, const char *name, void **dev, int64_t *count, int32_t *elem_bytes) {
+  if (!h || !name || !dev || !count || !elem_bytes) return fail(PCOM_ERR_ARG, "null argument");
+  Named f = lookup(h, name);
+  if (!f.p && !f.pf) return fail(PCOM_ERR_ARG, "unknown field '%s'", name);
+  *dev = f.p ? (void *)f.p : (void *)f.pf;
+  *count = f.n;
+  *elem_bytes = f.p ? 8 : 4;
+  return PCOM_OK;
 }
 
 int pcom_gpu_check_finite(pcom_handle *h) {

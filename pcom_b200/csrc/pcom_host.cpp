@@ -427,25 +427,43 @@ int pcom_model_destroy(pcom_model *m) {
 
 pcom_handle *pcom_model_handle(pcom_model *m) { return m ? m->h : nullptr; }
 
+int pcom_model_begin_step(pcom_model *M, int64_t *it, int32_t *new_day) {
+  if (!M || !it || !new_day) return PCOM_ERR_ARG;
+  if (!M->h) return PCOM_ERR_STATE;
+  M->iter += 1;
+  *it = M->iter;
+  *new_day = 0;
+  if (M->iter == 1 || M->ct.d != M->pt.d) {
+    // int_bnd on the device from the monthly fields uploaded at create
+    int m1, m2;
+    double f;
+    bnd_weights(*M, m1, m2, f);
+    M->nday += 1;
+    *new_day = 1;
+    int rc = pcom_gpu_int_bnd(M->h, m1, m2, f);
+    if (!rc) rc = pcom_gpu_den_prho(M->h);
+    if (rc) return rc;
+  }
+  return PCOM_OK;
+}
+
+int pcom_model_end_step(pcom_model *M) {
+  if (!M) return PCOM_ERR_ARG;
+  M->pt = M->ct;
+  M->ct = advance(M->ct, M->bc);
+  return PCOM_OK;
+}
+
 int pcom_model_run(pcom_model *M, int64_t nsteps) {
   if (!M) return PCOM_ERR_ARG;
   if (!M->h) return PCOM_ERR_STATE;
   for (int64_t n = 0; n < nsteps; ++n) {
-    M->iter += 1;
-    if (M->iter == 1 || M->ct.d != M->pt.d) {
-      // int_bnd on the device from the monthly fields uploaded at create
-      int m1, m2;
-      double f;
-      bnd_weights(*M, m1, m2, f);
-      M->nday += 1;
-      int rc = pcom_gpu_int_bnd(M->h, m1, m2, f);
-      if (!rc) rc = pcom_gpu_den_prho(M->h);
-      if (rc) return rc;
-    }
-    int rc = pcom_gpu_step(M->h, M->iter);
+    int64_t it = 0;
+    int32_t day = 0;
+    int rc = pcom_model_begin_step(M, &it, &day);
+    if (!rc) rc = pcom_gpu_step(M->h, it);
     if (rc) return rc;
-    M->pt = M->ct;
-    M->ct = advance(M->ct, M->bc);
+    pcom_model_end_step(M);
   }
   return PCOM_OK;
 }

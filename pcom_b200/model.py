@@ -98,6 +98,10 @@ class Model:
     def step_handle(self, tctr_i: int):
         L.check(self.lib.pcom_gpu_step(self.handle, int(tctr_i)), "pcom_gpu_step")
 
+    def set_rows(self, j_lo: int, j_hi: int):
+        """Rows the step's 3-D kernels compute (padded, 1-based; default all)."""
+        L.check(self.lib.pcom_gpu_set_rows(self.handle, int(j_lo), int(j_hi)), "set_rows")
+
     def check_finite(self):
         L.check(self.lib.pcom_gpu_check_finite(self.handle), "check_finite")
 
