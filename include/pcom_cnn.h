@@ -39,6 +39,8 @@ int64_t pcom_cnn_param_count(void);
 /* Buffers for up to max_images images of H x W. */
 int pcom_cnn_create(int32_t H, int32_t W, int32_t max_images, int32_t periodic_x, pcom_cnn **out);
 int pcom_cnn_destroy(pcom_cnn *c);
+/* Run on a caller's stream (stays the caller's: never destroyed here), or
+ * with stream = NULL on a new stream of the network's own. */
 int pcom_cnn_set_stream(pcom_cnn *c, void *stream);
 /* Host FP32 parameters in the layout above (resets the Adam moments). */
 int pcom_cnn_set_params(pcom_cnn *c, const float *params, int64_t n);

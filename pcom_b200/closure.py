@@ -259,51 +259,60 @@ VARIANTS = {  # applied fraction of each output (du, dv, dT, dS) and the |y| cli
     "tracers+0.25uv": ([0.25, 0.25, 1.0, 1.0], 3.0),
     "tracers-half": ([0.0, 0.0, 0.5, 0.5], 3.0),
 }
+# state fields pcom_gpu_coarsen sets (what a coarse run starts from)
+START_FIELDS = ("tc", "sc", "tp", "sp", "uc", "vc", "up", "vp", "auc", "aup", "aupp", "avc", "avp", "avpp",
+                "ubc", "vbc", "ubp", "vbp", "chc", "chp", "mch", "mch2", "am")
+FLAGS = {"fp64": L.PCOM_PREC_FP64, "fp64-fma": L.PCOM_FMA, "mixed": L.PCOM_PREC_MIXED,
+         "mixed-fma": L.PCOM_PREC_MIXED | L.PCOM_FMA}
 
 
-def evaluate(exp: Experiment, net: Network, steps: int, variants=VARIANTS):
-    """Coarse runs from CG(fine(t0)) beside the fine run for `steps` coarse
-    steps: the plain coarse model and, per variant, the model with the
-    closure applied after every step.  A closure run whose state stops being
-    finite falls back to the plain model (its state is replaced by the plain
-    run's and the closure is switched off).  RMS error against CG(fine(t))
-    at the end, and the time per step with and without the network."""
-    torch = exp.torch
-    plain = Model(exp.cc)
-    runs = {v: Model(exp.cc) for v in variants}
-    stats = {}
-    for v, (gain, clip) in variants.items():
-        st = dict(exp.stats, out_gain=gain, out_clip=clip)
-        stats[v] = _stats_struct(st)
-    for m in [plain] + list(runs.values()):
-        m.set_forcing(m.int_bnd())
+def coarse_run(exp: Experiment, flags: int) -> Model:
+    """A coarse model started from CG(fine(now)) in the given precision."""
+    m = Model(exp.cc, flags=flags)
+    m.set_forcing(m.int_bnd())
+    if flags & L.PCOM_PREC_MIXED:
+        exp.coarsen(exp.truth)
+        m.set_state(**{f: exp.truth.field(f) for f in START_FIELDS})
+    else:
         exp.coarsen(m)
+    return m
+
+
+def evaluate(exp: Experiment, net: Network, steps: int, forms: dict, flags: int = L.PCOM_PREC_FP64,
+             record_every: int = 24, plain_flags=(("plain", L.PCOM_PREC_FP64),)):
+    """Coarse runs from CG(fine(t0)) beside the fine run for `steps` coarse
+    steps: plain coarse models (`plain_flags`: name -> precision) and, per
+    form (name -> (gain, clip, cadence)), the model in precision `flags` with
+    the network's tendency applied every `cadence` steps over cadence x dt.
+    A closure run whose state stops being finite falls back to the plain
+    model (its state is replaced by the first plain run's and the closure is
+    switched off).  RMS error of u, v, T, S against CG(fine(t)) every
+    `record_every` steps and at the end."""
+    torch = exp.torch
+    plains = {n: coarse_run(exp, f) for n, f in plain_flags}
+    runs = {v: coarse_run(exp, flags) for v in forms}
+    stats = {v: _stats_struct(dict(exp.stats, out_gain=g, out_clip=c)) for v, (g, c, _) in forms.items()}
     x = torch.zeros((exp.npix, 16), dtype=torch.bfloat16, device="cuda")
     y = torch.zeros((exp.npix, 4), dtype=torch.float32, device="cuda")
-    active = {v: True for v in variants}
-    fallback = {v: None for v in variants}
+    active = {v: True for v in forms}
+    fallback = {v: None for v in forms}
+    hist = {n: [] for n in list(plains) + list(runs)}
+    first_plain = next(iter(plains.values()))
     it = 100
-    t_plain = t_net = 0.0
     for s in range(steps):
         it += 1
-        day = (s % 24 == 0)
-        t0 = time.perf_counter()
-        if day:
-            plain.den_prho()
-        plain.step_handle(it)
-        t_plain += time.perf_counter() - t0
-        for v, m in runs.items():
+        day = s % 24 == 0
+        for m in list(plains.values()) + list(runs.values()):
             if day:
                 m.den_prho()
             m.step_handle(it)
-            if active[v]:
-                t0 = time.perf_counter()
+        for v, m in runs.items():
+            cad = forms[v][2]
+            if active[v] and (s + 1) % cad == 0:
                 exp._features(m, x)
                 net.forward(x, y)
                 L.check(exp.lib.pcom_gpu_cnn_apply(m.handle, C.c_void_p(y.data_ptr()), C.byref(stats[v]),
-                                                   float(STEP)), "apply")
-                m.sync()
-                t_net += (time.perf_counter() - t0) / len(runs)
+                                                   float(STEP * cad)), "apply")
         if (s + 1) % 6 == 0 or s == steps - 1:
             for v, m in runs.items():
                 if not active[v]:
@@ -311,18 +320,71 @@ def evaluate(exp: Experiment, net: Network, steps: int, variants=VARIANTS):
                 try:
                     m.check_finite()
                 except L.PcomError:
-                    m.set_state(**{f: plain.field(f) for f in L.STATE_FIELDS})
+                    m.set_state(**{f: first_plain.field(f) for f in L.STATE_FIELDS})
                     active[v] = False
                     fallback[v] = s + 1
         exp.fine.run(exp.fine_steps)
-    res = dict(steps=steps, rms_plain=coarse_rms(exp, plain), s_per_step_plain=t_plain / steps,
-               s_per_step_network=t_net / steps, variants={})
-    for v, m in runs.items():
-        res["variants"][v] = dict(gain=variants[v][0], clip=variants[v][1], rms=coarse_rms(exp, m),
-                                  fell_back_at_step=fallback[v])
-    for m in [plain] + list(runs.values()):
+        if (s + 1) % record_every == 0 or s == steps - 1:
+            for n, m in list(plains.items()) + list(runs.items()):
+                hist[n].append(coarse_rms(exp, m))
+    mean = lambda h: {f: float(np.mean([r[f] for r in h])) for f in h[0]}
+    res = dict(steps=steps, record_every=record_every, plain={}, forms={})
+    for n in plains:
+        res["plain"][n] = dict(rms_end=hist[n][-1], rms_mean=mean(hist[n]))
+    for v in runs:
+        g, c, cad = forms[v]
+        res["forms"][v] = dict(gain=g, clip=c, cadence=cad, rms_end=hist[v][-1], rms_mean=mean(hist[v]),
+                               fell_back_at_step=fallback[v])
+    for m in list(plains.values()) + list(runs.values()):
         m.close()
     return res
+
+
+def form_cost(exp: Experiment, net: Network, flags: int, steps: int = 48) -> dict:
+    """Device time of a coarse step in precision `flags` and of one closure
+    application (features, forward, apply), CUDA events."""
+    torch = exp.torch
+    m = coarse_run(exp, flags)
+    s = torch.cuda.current_stream()
+    m.set_stream(s.cuda_stream)
+    net.set_stream(s.cuda_stream)
+    st = _stats_struct(dict(exp.stats, out_gain=[0.0, 0.0, 0.0, 0.0], out_clip=3.0))
+    x = torch.zeros((exp.npix, 16), dtype=torch.bfloat16, device="cuda")
+    y = torch.zeros((exp.npix, 4), dtype=torch.float32, device="cuda")
+    lib = exp.lib
+
+    def net_once():
+        L.check(lib.pcom_gpu_cnn_features(m.handle, C.c_void_p(x.data_ptr()), C.byref(st)), "features")
+        net.forward(x, y)
+        L.check(lib.pcom_gpu_cnn_apply(m.handle, C.c_void_p(y.data_ptr()), C.byref(st), float(STEP)), "apply")
+
+    it = 100
+    for _ in range(3):
+        it += 1
+        L.check(lib.pcom_gpu_step_async(m.handle, it), "step")
+        net_once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        it += 1
+        L.check(lib.pcom_gpu_step_async(m.handle, it), "step")
+    e1.record(s)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / steps
+    e0.record(s)
+    for _ in range(steps // 4):
+        net_once()
+    e1.record(s)
+    torch.cuda.synchronize()
+    net_ms = e0.elapsed_time(e1) / (steps // 4)
+    m.close()
+    net.set_stream(0)
+    return dict(step_ms=round(step_ms, 4), network_ms=round(net_ms, 4))
+
+
+def sypd_of(ms_per_step: float) -> float:
+    return (86400.0 / (ms_per_step / 1000.0)) * STEP / (365 * 86400.0)
 
 
 def main():
@@ -330,20 +392,29 @@ def main():
 
     p = argparse.ArgumentParser()
     p.add_argument("--fine", default="global025")
+    p.add_argument("--fine-flags", default="fp64", choices=sorted(FLAGS))
     p.add_argument("--factor", type=int, default=4)
     p.add_argument("--spinup-days", type=float, default=2)
     p.add_argument("--train-days", type=float, default=8)
-    p.add_argument("--every", type=int, default=2)
+    p.add_argument("--every", type=int, default=2, help="coarse steps between training samples")
     p.add_argument("--target-steps", type=int, default=1,
                    help="coarse steps the training residual is accumulated over")
-    p.add_argument("--eval-days", type=float, default=2)
+    p.add_argument("--val-days", type=float, default=2, help="window that picks the applied outputs and gain")
+    p.add_argument("--test-days", type=float, default=2, help="window the chosen closure is judged on")
+    p.add_argument("--form-flags", default="fp64", choices=sorted(FLAGS),
+                   help="precision of the closure form's coarse model")
+    p.add_argument("--cadences", default="1", help="comma-separated: apply the network every k coarse steps")
     p.add_argument("--epochs", type=int, default=8)
     p.add_argument("--lr", type=float, default=1e-3)
     p.add_argument("--out", default=None)
     a = p.parse_args()
     torch.cuda.set_device(0)
     t0 = time.time()
-    exp = Experiment(make_case(a.fine), a.factor, a.target_steps)
+    fc = make_case(a.fine)
+    exp = Experiment(fc, a.factor, a.target_steps)
+    if FLAGS[a.fine_flags] != L.PCOM_PREC_FP64:
+        exp.fine.close()
+        exp.fine = Model(fc, flags=FLAGS[a.fine_flags])
     fine_spd = 86400 // exp.fc["dtbc"]
     tf = time.perf_counter()
     exp.fine.run(int(a.spinup_days * fine_spd))
@@ -356,10 +427,32 @@ def main():
     tt = time.perf_counter()
     tr = train(net, xs, ts, mask, a.epochs, a.lr)
     t_train = time.perf_counter() - tt
-    ev = evaluate(exp, net, int(a.eval_days * 24))
-    res = dict(fine=a.fine, coarse_grid=[exp.W, exp.H, exp.nk], samples=nsamp, epochs=a.epochs,
-               target_steps=a.target_steps,
-               train=tr, train_seconds=t_train, eval=ev, stats=exp.stats, fine_s_per_step=fine_s_per_step,
+    del xs, ts
+    torch.cuda.empty_cache()
+    # validation window: which outputs, at which gain (every step, FP64)
+    val = evaluate(exp, net, int(a.val_days * 24), {v: (g, c, 1) for v, (g, c) in VARIANTS.items()})
+    score = lambda r: r["rms_mean"]["tc"] / max(val["plain"]["plain"]["rms_mean"]["tc"], 1e-30)
+    best = min(val["forms"], key=lambda v: score(val["forms"][v]))
+    g, c = VARIANTS[best]
+    # test window: the chosen closure at each cadence in the form's precision,
+    # beside the plain model in FP64 and in the form's precision
+    cads = [int(x) for x in a.cadences.split(",")]
+    forms = {f"{best}@{k}": (g, c, k) for k in cads}
+    plains = (("plain", L.PCOM_PREC_FP64),) + ((("plain_" + a.form_flags, FLAGS[a.form_flags]),)
+                                               if a.form_flags != "fp64" else ())
+    test = evaluate(exp, net, int(a.test_days * 24), forms, FLAGS[a.form_flags], plain_flags=plains)
+    cost_fp64 = form_cost(exp, net, L.PCOM_PREC_FP64)
+    cost_form = form_cost(exp, net, FLAGS[a.form_flags])
+    test["sypd"] = {"plain": round(sypd_of(cost_fp64["step_ms"]), 1)}
+    if a.form_flags != "fp64":
+        test["sypd"]["plain_" + a.form_flags] = round(sypd_of(cost_form["step_ms"]), 1)
+    for k in cads:
+        test["sypd"][f"{best}@{k}"] = round(sypd_of(cost_form["step_ms"] + cost_form["network_ms"] / k), 1)
+    res = dict(fine=a.fine, fine_flags=a.fine_flags, coarse_grid=[exp.W, exp.H, exp.nk], samples=nsamp,
+               every=a.every, epochs=a.epochs, target_steps=a.target_steps, spinup_days=a.spinup_days,
+               train_days=a.train_days, val_days=a.val_days, test_days=a.test_days, form_flags=a.form_flags,
+               train=tr, train_seconds=t_train, validation=val, chosen=best, test=test,
+               cost={"fp64": cost_fp64, a.form_flags: cost_form}, stats=exp.stats, fine_s_per_step=fine_s_per_step,
                fine_steps_per_coarse_step=exp.fine_steps, wall_seconds=time.time() - t0)
     line = json.dumps(res)
     print(line)

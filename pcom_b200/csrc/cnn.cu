@@ -127,6 +127,7 @@ __global__ void k_zero_pad(float *w1, float *w5, float *b5) {
 struct pcom_cnn {
   int H = 0, W = 0, max_img = 0, periodic_x = 1;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;  // created here (destroyed here), or the caller's
   long long nparam = 0;
   float *param = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;  // FP32, [W1 b1 ... W5 b5]
   __nv_bfloat16 *wf[kLayers] = {}, *wd[kLayers] = {};                   // operand copies
@@ -277,19 +278,23 @@ int pcom_cnn_destroy(pcom_cnn *c) {
   if (!c) return PCOM_CNN_OK;
   cudaStreamSynchronize(c->stream);
   cudaStream_t s = c->stream;
+  const bool own = c->own_stream;
   delete c;
-  cudaStreamDestroy(s);
+  if (own) cudaStreamDestroy(s);
   return PCOM_CNN_OK;
 }
 
 int pcom_cnn_set_stream(pcom_cnn *c, void *stream) {
   if (!c) return cfail(PCOM_CNN_ERR_ARG, "null network");
   CC(cudaStreamSynchronize(c->stream));
-  cudaStreamDestroy(c->stream);
+  // only a stream this network created is destroyed; a caller's stays theirs
+  if (c->own_stream) cudaStreamDestroy(c->stream);
   if (stream) {
     c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
   } else {
     CC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
   }
   return PCOM_CNN_OK;
 }

@@ -203,7 +203,8 @@ struct Grid2 {
   int ni, glo_ni, glo_nj, nk;
   long long n2;
 };
-__device__ __forceinline__ void put_twin(double *f, const Grid2 &g, int i, long long q, double v) {
+template <typename T>
+__device__ __forceinline__ void put_twin(T *f, const Grid2 &g, int i, long long q, T v) {
   f[q] = v;
   if (i == 2) f[q + (g.ni - 2)] = v;
   else if (i == g.ni - 1) f[q - (g.ni - 2)] = v;
@@ -238,18 +239,22 @@ struct CnnStatsDev {
   double alpha_ref[64];
 };
 __device__ __forceinline__ float clip_y(float y, float c) { return c > 0.f ? fminf(fmaxf(y, -c), c) : y; }
-__global__ void k_cnn_features(const __grid_constant__ Dev P, __nv_bfloat16 *x, CnnStatsDev st) {
+// R: the handle's 3-D storage (the mixed path stores alpha as alpha - alpha_r(k))
+template <typename R>
+__global__ void k_cnn_features(const __grid_constant__ DevT<R> P, __nv_bfloat16 *x, CnnStatsDev st) {
+  constexpr bool MIXED = std::is_same<R, float>::value;
   const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
     const int I = (int)(p % P.glo_ni), J = (int)((p / P.glo_ni) % P.glo_nj), k = (int)(p / ((long long)P.glo_ni * P.glo_nj)) + 1;
     const long long q2 = (long long)(I + 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
     const bool wu = P.lev_u[q2] >= k, wt = P.lev_t[q2] >= k;
     float v[5];
-    v[0] = wu ? (float)((P.uc[q] - st.in_mean[0]) / st.in_std[0]) : 0.f;
-    v[1] = wu ? (float)((P.vc[q] - st.in_mean[1]) / st.in_std[1]) : 0.f;
-    v[2] = wt ? (float)((P.tc[q] - st.in_mean[2]) / st.in_std[2]) : 0.f;
-    v[3] = wt ? (float)((P.sc[q] - st.in_mean[3]) / st.in_std[3]) : 0.f;
-    v[4] = wt ? (float)((P.alpha[q] - st.alpha_ref[k - 1] - st.in_mean[4]) / st.in_std[4]) : 0.f;
+    const double al = MIXED ? (double)P.alpha[q] + P.alpha_r[k] : (double)P.alpha[q];
+    v[0] = wu ? (float)(((double)P.uc[q] - st.in_mean[0]) / st.in_std[0]) : 0.f;
+    v[1] = wu ? (float)(((double)P.vc[q] - st.in_mean[1]) / st.in_std[1]) : 0.f;
+    v[2] = wt ? (float)(((double)P.tc[q] - st.in_mean[2]) / st.in_std[2]) : 0.f;
+    v[3] = wt ? (float)(((double)P.sc[q] - st.in_mean[3]) / st.in_std[3]) : 0.f;
+    v[4] = wt ? (float)((al - st.alpha_ref[k - 1] - st.in_mean[4]) / st.in_std[4]) : 0.f;
     __nv_bfloat16 *o = x + p * 16;
     #pragma unroll
     for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16(c < 5 ? v[c] : 0.f);
@@ -276,7 +281,8 @@ __global__ void k_cnn_target(const __grid_constant__ Dev Pp, const __grid_consta
     }
   }
 }
-__global__ void k_cnn_apply(const __grid_constant__ Dev P, const float *y, CnnStatsDev st, double dt, int tp_distinct) {
+template <typename R>
+__global__ void k_cnn_apply(const __grid_constant__ DevT<R> P, const float *y, CnnStatsDev st, double dt, int tp_distinct) {
   const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
   const Grid2 G{P.ni, P.glo_ni, P.glo_nj, P.nk, P.n2};
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
@@ -286,19 +292,19 @@ __global__ void k_cnn_apply(const __grid_constant__ Dev P, const float *y, CnnSt
     if (P.lev_u[q2] >= k) {
       const double du = dt * st.out_gain[0] * st.out_std[0] * clip_y(y[p * 4 + 0], st.out_clip);
       const double dv = dt * st.out_gain[1] * st.out_std[1] * clip_y(y[p * 4 + 1], st.out_clip);
-      put_twin(P.uc, G, i, q, P.uc[q] + du);
-      put_twin(P.vc, G, i, q, P.vc[q] + dv);
-      put_twin(P.up, G, i, q, P.up[q] + du);
-      put_twin(P.vp, G, i, q, P.vp[q] + dv);
+      put_twin(P.uc, G, i, q, (R)(P.uc[q] + du));
+      put_twin(P.vc, G, i, q, (R)(P.vc[q] + dv));
+      put_twin(P.up, G, i, q, (R)(P.up[q] + du));
+      put_twin(P.vp, G, i, q, (R)(P.vp[q] + dv));
     }
     if (P.lev_t[q2] >= k) {
       const double dT = dt * st.out_gain[2] * st.out_std[2] * clip_y(y[p * 4 + 2], st.out_clip);
       const double dS = dt * st.out_gain[3] * st.out_std[3] * clip_y(y[p * 4 + 3], st.out_clip);
-      put_twin(P.tc, G, i, q, P.tc[q] + dT);
-      put_twin(P.sc, G, i, q, P.sc[q] + dS);
+      put_twin(P.tc, G, i, q, (R)(P.tc[q] + dT));
+      put_twin(P.sc, G, i, q, (R)(P.sc[q] + dS));
       if (tp_distinct) {
-        put_twin(P.tp, G, i, q, P.tp[q] + dT);
-        put_twin(P.sp, G, i, q, P.sp[q] + dS);
+        put_twin(P.tp, G, i, q, (R)(P.tp[q] + dT));
+        put_twin(P.sp, G, i, q, (R)(P.sp[q] + dS));
       }
     }
   }
@@ -1572,8 +1578,8 @@ int pcom_gpu_coarsen(pcom_handle *f, pcom_handle *c, int32_t factor) {
 
 int pcom_gpu_cnn_features(pcom_handle *h, void *x, const pcom_cnn_stats *st) {
   if (!h || !x || !st) return fail(PCOM_ERR_ARG, "null argument");
-  if (h->mixed) return fail(PCOM_ERR_ARG, "closure features are built from FP64 handles");
-  k_cnn_features<<<592, 256, 0, h->stream>>>(h->D, (__nv_bfloat16 *)x, stats_dev(st));
+  if (h->mixed) k_cnn_features<float><<<592, 256, 0, h->stream>>>(h->DM, (__nv_bfloat16 *)x, stats_dev(st));
+  else k_cnn_features<double><<<592, 256, 0, h->stream>>>(h->D, (__nv_bfloat16 *)x, stats_dev(st));
   CK(cudaGetLastError());
   h->launches++;
   return PCOM_OK;
@@ -1593,8 +1599,10 @@ int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, fl
 
 int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *st, double dt) {
   if (!h || !y || !st) return fail(PCOM_ERR_ARG, "null argument");
-  if (h->mixed) return fail(PCOM_ERR_ARG, "the closure is applied on FP64 handles");
-  k_cnn_apply<<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
+  if (h->mixed)
+    k_cnn_apply<float><<<592, 256, 0, h->stream>>>(h->DM, y, stats_dev(st), dt, h->DM.tp != h->DM.tc ? 1 : 0);
+  else
+    k_cnn_apply<double><<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
   CK(cudaGetLastError());
   h->launches++;
   return PCOM_OK;

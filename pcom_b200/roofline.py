@@ -81,12 +81,12 @@ def _steps(m, first: int, n: int, day_of):
         L.check(lib.pcom_gpu_step_async(m.handle, it), "step")
 
 
-def kernel_table(case: dict, mixed: bool, steps: int) -> dict:
+def kernel_table(case: dict, mixed: bool, steps: int, fma: bool = False) -> dict:
     import torch
 
     from .model import Model
 
-    m = Model(case, flags=L.PCOM_PREC_MIXED if mixed else L.PCOM_PREC_FP64)
+    m = Model(case, flags=(L.PCOM_PREC_MIXED if mixed else L.PCOM_PREC_FP64) | (L.PCOM_FMA if fma else 0))
     m.run(3)  # AB3 start-up and a warm cache of kernels
     spd = 86400 // case["dtbc"]
     day_of = lambda it: (it - 1) // spd
@@ -150,6 +150,43 @@ def days_run(case: dict, days: float) -> dict:
     return out
 
 
+def cnn_table(H: int, W: int, nimg: int, steps: int) -> dict:
+    """The closure network on nimg images of H x W (one per level of a
+    H x W grid): CUDA-event time of the forward pass and of a training step
+    (forward, data and weight gradients, Adam) on random inputs, and their
+    tensor throughput on the FLOPs the convolutions issue (padded channels)."""
+    import torch
+
+    from .closure import Network
+
+    net = Network(H, W, nimg, seed=5)
+    npix = H * W * nimg
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.zeros((npix, 16), dtype=torch.bfloat16, device="cuda")
+    x[:, :5] = torch.randn((npix, 5), generator=g, device="cuda").to(torch.bfloat16)
+    y = torch.zeros((npix, 4), dtype=torch.float32, device="cuda")
+    t = torch.randn((npix, 4), generator=g, device="cuda")
+    mk = torch.ones((npix, 4), device="cuda")
+    s = torch.cuda.current_stream()
+    net.set_stream(s.cuda_stream)
+    flop = npix * 9 * 2 * (16 * 64 + 3 * 64 * 64 + 64 * 16)
+    out = {"images": nimg, "H": H, "W": W, "flop_per_forward": flop}
+    for name, fn in (("forward", lambda: net.forward(x, y)), ("train_step", lambda: net.train_step(x, t, mk, 1e-4))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        f = flop * (3 if name == "train_step" else 1)
+        out[name] = {"ms": round(ms, 4), "TFLOP_s": round(f / (ms * 1e-3) / 1e12, 1)}
+    net.close()
+    return out
+
+
 def markdown(rep: dict) -> str:
     lines = []
     for name in ("fp64", "mixed"):
@@ -180,12 +217,18 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=12, help="steps timed per path (and again with events)")
     ap.add_argument("--days", type=float, default=0.0, help="model days of the time loop on both paths")
     ap.add_argument("--json", default=None)
+    ap.add_argument("--fma", action="store_true", help="the PCOM_FMA builds of the step kernels")
+    ap.add_argument("--cnn", type=int, default=0, help="also time N forward passes and training steps of the "
+                                                      "closure network on the case's level images")
     a = ap.parse_args(argv)
     case = make_case(a.case)
     rep = {"case": a.case, "grid": [case["glo_ni"], case["glo_nj"], case["nk"]], "steps": a.steps,
-           "fp64": kernel_table(case, False, a.steps), "mixed": kernel_table(case, True, a.steps)}
+           "fp64": kernel_table(case, False, a.steps, a.fma), "mixed": kernel_table(case, True, a.steps, a.fma)}
     if a.days > 0:
         rep["days_run"] = days_run(case, a.days)
+    if a.cnn > 0:
+        rep["cnn"] = cnn_table(case["glo_nj"], case["glo_ni"], case["nk"], a.cnn)
+        print(json.dumps(rep["cnn"]))
     if a.json:
         with open(a.json, "w") as f:
             json.dump(rep, f, indent=1)
