@@ -21,10 +21,14 @@
 // Every wait is bounded: a timed-out mbarrier wait sets the error flag,
 // waits (bounded) once more for the MMAs in flight, frees tensor memory and
 // returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
+
+#include <cudaTypedefs.h>
 
 #include "cnn_kernels.h"
 
@@ -244,73 +248,126 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__res
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
 
-// ----------------------------------------------------------------------------
-// Persistent form of the same convolution.  A tile is 128 consecutive pixels
-// of one image row.  Each CTA walks a contiguous strip of tiles down the rows
-// of one column of tiles, so consecutive tiles share two of their three halo
-// rows: the halo rows live in a ring of 4 slots in shared memory
-// "chunk-planar" (plane c holds channels 8c..8c+7, 16 bytes per pixel, a
-// slot's 130 pixels contiguous), and each tile loads one new row.  The A
-// operand of tap (dy, dx) is the planes of the slot holding row y + dy read
-// from pixel dx + 1: leading byte offset = plane size (K direction), stride
-// byte offset = 128 bytes (8 pixels).  Taps whose row falls outside the
-// image are skipped (their contribution is zero).  All 9 taps of the weights
-// stay in shared memory for the kernel's lifetime.
-//
-// Two accumulators in tensor memory: the MMAs of tile i+1 are issued as soon
-// as those of tile i complete, so the tensor cores work on tile i+1 while the
-// CTA drains tile i's accumulator and loads the row tile i+2 adds.  Warps w
-// and w+4 read lane quarter w%4 of the accumulator, each half of its columns.
+// Ring geometry of the persistent convolution below: a tile is 128
+// consecutive pixels of one image row, its halo rows hold 130 pixels, stored
+// "chunk-planar" (plane c holds channels 8c..8c+7, 16 bytes per pixel).
 constexpr int kHaloW = kM + 2;               // halo columns
-constexpr int kRing = 4;                     // halo row slots
 constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 bytes)
-constexpr int kRPlane = kRing * kRowB;       // one 8-channel plane of the ring
-constexpr int kHThreads = 256;               // 8 warps: two per TMEM lane quarter
+
+// ----------------------------------------------------------------------------
+// Persistent convolution (the form every whole-image convolution takes).
+// Each CTA walks a contiguous strip of tiles down the rows of one column of
+// tiles, so consecutive tiles share two of their three halo rows: the rows
+// live in a ring of slots, each tile loads one new row, and the A operand of
+// tap (dy, dx) is the planes of the slot holding row y + dy read from pixel
+// dx + 1 (leading byte offset = plane stride, stride byte offset = 128 bytes
+// = 8 pixels).  Taps whose row falls outside the image are skipped.  All 9
+// taps of the weights stay in shared memory.  Two accumulators in tensor
+// memory let the MMAs of one tile run while the previous one is drained.
+// Each role has its own warps and
+// they hand work to one another through mbarriers instead of CTA barriers
+// (six ring slots instead of four, so row loads run up to three tiles ahead):
+//   warps 0-3  epilogue: warp w drains lane quarter w of an accumulator
+//              (tcgen05.ld), frees it, applies bias + ReLU (or the ReLU mask)
+//              and stores the tile; 64-channel BF16 tiles go through a
+//              double-buffered staging tile in the 128-byte swizzled layout
+//              and leave with one TMA tensor store (cp.async.bulk.tensor)
+//   warp 4     loads: streams each new halo row into its ring slot with
+//              cp.async, whose completion arrives on the slot's "full"
+//              mbarrier; reuses a slot once the MMAs reading its old row
+//              have completed ("empty" mbarrier, tcgen05.commit)
+//   warp 5     MMA: one thread waits for the tile's rows and a free
+//              accumulator, issues the 9 taps x CIN/16 MMAs and commits
+//              "accumulator full" and the release of the rows the next tile
+//              does not read.
+// The plane stride of the ring is padded by 16 bytes so a load warp's eight
+// 16-byte chunks of one pixel land in different banks.  Every wait is
+// bounded: a wait that gives up sets the error flag and a shared stop flag,
+// and every role leaves its loop; the MMA thread then waits (bounded) for its
+// MMAs before tensor memory is freed.
+constexpr int kWsThreads = 192;
+constexpr int kWsRing = 6;                     // halo row slots: loads run up to three tiles ahead
+constexpr int kPlaneW = kWsRing * kRowB + 16;  // padded ring plane (12,496 bytes)
+
+__device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void tma_store3(const CUtensorMap *map, uint32_t src, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(map),
+               "r"(src), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 template <int CIN, int NOUT>
-__global__ void __launch_bounds__(kHThreads) k_conv_halo(const __nv_bfloat16 *__restrict__ in,
-                                                         const __nv_bfloat16 *__restrict__ w,
-                                                         const float *__restrict__ bias,
-                                                         const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
-                                                         int H, int W, int periodic_x, int mode, int nstore, int *err) {
+__host__ __device__ constexpr bool ws_tma() { return NOUT == 64; }
+
+template <int CIN, int NOUT>
+__global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__restrict__ in,
+                                                        const __nv_bfloat16 *__restrict__ w,
+                                                        const float *__restrict__ bias,
+                                                        const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
+                                                        int H, int W, int periodic_x, int mode, int nstore, int *err,
+                                                        const __grid_constant__ CUtensorMap tmap) {
   constexpr int KC = CIN / 8;
   constexpr int W_BYTES = 9 * NOUT * CIN * 2;
-  constexpr int A_BYTES = KC * kRPlane;
-  constexpr int ROWB = NOUT * 2 + 16;  // padded BF16 row of the output staging tile
+  constexpr int STG = kM * NOUT * 2;  // one staging tile
   constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
-  constexpr int NSPLIT = NOUT >= 32 ? 2 : 1;  // warps sharing a lane quarter's columns
-  constexpr int CPW = NOUT / NSPLIT;          // accumulator columns per warp
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t mbar[2];  // MMAs of accumulator b done
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full[kWsRing], empty[kWsRing], accf[2], acce[2], sfree[2], swritten[2], done;
   __shared__ uint32_t tmem_slot;
+  __shared__ volatile int s_stop;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const int quarter = warp & 3, half = warp >> 2;
-  uint8_t *Wsm = smem, *Ring = smem + W_BYTES, *Osm = smem + W_BYTES + A_BYTES;
+  // 1024-byte aligned base: the swizzled staging tiles need it
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  uint8_t *const sbase = smem_raw + (base - smem_u32(smem_raw));
+  const bool tma = ws_tma<CIN, NOUT>() && mode != 1;
+  const uint32_t Stg = base, Wsm = base + (ws_tma<CIN, NOUT>() ? 2 * STG : 0), Ring = Wsm + W_BYTES;
+  uint8_t *const stg_p = sbase;
   const int ntx = (W + kM - 1) / kM;
-  const long long NR = (long long)nimg * H;  // image rows
+  const long long NR = (long long)nimg * H;
   const long long ntiles = NR * ntx;
-  // this CTA's strip: tiles t0..t1-1, t = tx * NR + (img * H + y)
   const long long chunk = (ntiles + gridDim.x - 1) / gridDim.x;
   const long long t0 = (long long)blockIdx.x * chunk;
   const long long t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
 
   if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), 2 * NCOLS);
   if (tid == 0) {
-    mbar_init(smem_u32(&mbar[0]), 1);
-    mbar_init(smem_u32(&mbar[1]), 1);
+    for (int q = 0; q < kWsRing; ++q) {
+      mbar_init(smem_u32(&full[q]), 32);  // one arrival per load-warp lane
+      mbar_init(smem_u32(&empty[q]), 1);
+    }
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(smem_u32(&accf[q]), 1);
+      mbar_init(smem_u32(&acce[q]), 4);        // one per epilogue warp
+      mbar_init(smem_u32(&sfree[q]), 1);       // staging tile q read by its last store
+      mbar_init(smem_u32(&swritten[q]), 128);  // staging tile q written by the epilogue
+    }
+    mbar_init(smem_u32(&done), 1);
+    s_stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // weights: tap t, core matrix (n/8, c) at t*NOUT*CIN*2 + ((n/8)*KC + c)*128 + (n%8)*16
-  for (int q = tid; q < 9 * NOUT * KC; q += kHThreads) {
+  // weights (all threads), resident for the kernel's lifetime
+  for (int q = tid; q < 9 * NOUT * KC; q += kWsThreads) {
     const int t = q / (NOUT * KC), r = q % (NOUT * KC), n = r / KC, c = r % KC;
-    const uint32_t dst = smem_u32(Wsm) + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16);
-    cp_async16(dst, w + ((long long)t * NOUT + n) * CIN + c * 8, true);
+    cp_async16(Wsm + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16),
+               w + ((long long)t * NOUT + n) * CIN + c * 8, true);
   }
-  // a tile's position: column tile, image row gr = img * H + y, and y
+  cp_async_wait_all();
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
   struct Pos {
     int tx, gr, y;
   };
-  // the tile after `a` in t order (rows first, then column tiles)
   auto advance = [&](Pos a) {
     ++a.gr;
     if (++a.y == H) a.y = 0;
@@ -321,216 +378,216 @@ __global__ void __launch_bounds__(kHThreads) k_conv_halo(const __nv_bfloat16 *__
     }
     return a;
   };
-  // ring bookkeeping, identical in every thread: slot s holds image row
-  // tag_row[s] of column tile tag_tx[s]
-  int tag_row[kRing] = {-1, -1, -1, -1};
-  int tag_tx[kRing] = {-1, -1, -1, -1};
-  // row gr (= img * H + y) of column tile tx into slot gr % 4 (cp.async)
-  auto load_row = [&](int tx, int gr) {
-    const int s = gr & 3;
-    const int x0 = tx * kM;
-    for (int q = tid; q < kHaloW * KC; q += kHThreads) {
-      const int u = q / KC, c = q % KC;
-      int xx = x0 - 1 + u;
-      bool ok = true;
-      if (xx < 0 || xx >= W) {
-        if (periodic_x) {
-          if (xx < 0) xx += W;  // x0 - 1 >= -1
-          else if ((xx -= W) >= W) xx %= W;
-        } else {
-          ok = false;
-        }
-      }
-      const uint32_t dst = smem_u32(Ring) + (uint32_t)(c * kRPlane + s * kRowB + u * 16);
-      cp_async16(dst, ok ? (const void *)(in + ((long long)gr * W + xx) * CIN + c * 8) : (const void *)in, ok);
-    }
-    tag_row[s] = gr;
-    tag_tx[s] = tx;
-  };
-  // the image rows a tile reads: y - 1, y, y + 1 inside the image
   auto row_used = [&](const Pos &a, int dy) { return a.y + dy >= 0 && a.y + dy < H; };
-  // whether the rows of tile `a` missing from the ring go to slots that tile
-  // `busy` (whose MMAs may be in flight) does not read
-  auto can_load = [&](const Pos &a, const Pos &busy) {
-    for (int dy = -1; dy <= 1; ++dy) {
-      if (!row_used(a, dy)) continue;
-      const int s = (a.gr + dy) & 3;
-      if (tag_row[s] == a.gr + dy && tag_tx[s] == a.tx) continue;
-      for (int by = -1; by <= 1; ++by)
-        if (row_used(busy, by) && ((busy.gr + by) & 3) == s) return false;
-    }
-    return true;
-  };
-  auto ensure_rows = [&](const Pos &a) {
-    for (int dy = -1; dy <= 1; ++dy) {
-      if (!row_used(a, dy)) continue;
-      const int s = (a.gr + dy) & 3;
-      if (!(tag_row[s] == a.gr + dy && tag_tx[s] == a.tx)) load_row(a.tx, a.gr + dy);
-    }
-  };
-  constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
-  // descriptors with the start address at the ring and at the weights; the
-  // others differ only in the start address field (address >> 4 in the low
-  // 14 bits; shared memory addresses stay below 256 KB, so it never carries)
-  const uint64_t adesc0 = umma_desc(smem_u32(Ring), kRPlane, 128);
-  const uint64_t bdesc0 = umma_desc(smem_u32(Wsm), 128, KC * 128);
-  // the taps of tile `a` inside the image x CIN/16 K-steps into accumulator
-  // `acc` (one thread)
-  auto issue_mma = [&](const Pos &a, uint32_t acc, uint32_t mb) {
-    tc_fence_after();
-    uint32_t accum = 0;
-    #pragma unroll
-    for (int tp = 0; tp < 9; ++tp) {
-      const int dy = tp / 3 - 1, dx = tp % 3 - 1;
-      if (!row_used(a, dy)) continue;
-      const int s = (a.gr + dy) & 3;
-      #pragma unroll
-      for (int j = 0; j < CIN / 16; ++j) {
-        const uint64_t ad = adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kRPlane) >> 4);
-        const uint64_t bd = bdesc0 + (uint64_t)((tp * NOUT * CIN * 2 + j * 256) >> 4);
-        umma_bf16(acc, ad, bd, idesc, accum);
-        accum = 1u;
-      }
-    }
-    umma_commit(mb);
-  };
-  uint32_t ph[2] = {0, 0};
-  bool mpend = false;  // an MMA group issued and not yet waited for
-  int mpend_b = 0;
-  bool fail = false;
-  bool deferred = false;  // the next tile's rows are loaded after the current tile's MMAs
-  long long tile = t0;
-  // positions of tiles tile, tile + 1, tile + 2
-  Pos p0{0, 0, 0};
+  Pos first{0, 0, 0};
   if (t0 < t1) {
-    p0.tx = (int)(t0 / NR);
-    p0.gr = (int)(t0 % NR);
-    p0.y = p0.gr % H;
+    first.tx = (int)(t0 / NR);
+    first.gr = (int)(t0 % NR);
+    first.y = first.gr % H;
   }
-  Pos p1 = advance(p0), p2 = advance(p1);
-  if (tile < t1) ensure_rows(p0);
-  cp_async_wait_all();  // the weights and the first tile's rows
-  fence_async_smem();
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = tmem_slot;
-  if (tile < t1) {
-    if (tid == 0) issue_mma(p0, tmem, smem_u32(&mbar[0]));
-    mpend = true;
-    mpend_b = 0;
-    if (tile + 1 < t1) {
-      if (can_load(p1, p0)) ensure_rows(p1);
-      else deferred = true;
-    }
-  }
-  for (int it = 0; tile < t1; ++tile, ++it, p0 = p1, p1 = p2, p2 = advance(p2)) {
-    const int b = it & 1;
-    cp_async_wait_all();  // the next tile's rows (issued one tile earlier)
-    fence_async_smem();
-    const bool done = mbar_wait(smem_u32(&mbar[b]), ph[b]);  // this tile's MMAs
-    if (__syncthreads_or(!done)) {
-      fail = true;
-      break;
-    }
-    ph[b] ^= 1;
-    mpend = false;
-    const bool next = tile + 1 < t1;
-    if (next && deferred) {
-      // the ring slots are free now: load, wait and publish the next rows
-      ensure_rows(p1);
-      cp_async_wait_all();
-      fence_async_smem();
-      __syncthreads();
-      deferred = false;
-    }
-    tc_fence_after();
-    if (next) {
-      if (tid == 0) issue_mma(p1, tmem + (uint32_t)(1 - b) * NCOLS, smem_u32(&mbar[1 - b]));
-      mpend = true;
-      mpend_b = 1 - b;
-      // rows of tile + 2, into slots tile + 1 does not read
-      if (tile + 2 < t1) {
-        if (can_load(p2, p1)) ensure_rows(p2);
-        else deferred = true;
+  auto stop = [&]() {
+    s_stop = 1;
+    atomicExch(err, 1);
+  };
+
+  if (warp == 4) {
+    // ---------------------------------------------------------------- loads
+    int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
+    for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
+    Pos a = first;
+    for (long long tile = t0; tile < t1 && !s_stop; ++tile, a = advance(a)) {
+      for (int dy = -1; dy <= 1; ++dy) {
+        if (!row_used(a, dy)) continue;
+        const int r = a.gr + dy, s = r % kWsRing;
+        if (tag_row[s] == r && tag_tx[s] == a.tx) continue;
+        // the slot's previous row is free once the MMAs that read it are done
+        if (nload[s] > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((nload[s] - 1) & 1))) {
+          stop();
+          break;
+        }
+        const int x0 = a.tx * kM;
+        for (int q = lane; q < kHaloW * KC; q += 32) {
+          const int u = q / KC, c = q % KC;
+          int xx = x0 - 1 + u;
+          bool ok = true;
+          if (xx < 0 || xx >= W) {
+            if (periodic_x) {
+              if (xx < 0) xx += W;
+              else if ((xx -= W) >= W) xx %= W;
+            } else {
+              ok = false;
+            }
+          }
+          cp_async16(Ring + (uint32_t)(c * kPlaneW + s * kRowB + u * 16),
+                     ok ? (const void *)(in + ((long long)r * W + xx) * CIN + c * 8) : (const void *)in, ok);
+        }
+        cp_async_arrive_noinc(smem_u32(&full[s]));
+        tag_row[s] = r;
+        tag_tx[s] = a.tx;
+        ++nload[s];
       }
     }
-    const uint32_t acc = tmem + (uint32_t)b * NCOLS;
-    const int tx = p0.tx;
-    const long long row = p0.gr;
-    const int m = quarter * 32 + lane, x0 = tx * kM, x = x0 + m;
-    const int nvalid = min(kM, W - x0);
-    const long long p = row * W + x;
-    const uint32_t lane_addr = acc + ((uint32_t)(quarter * 32) << 16);
-    if (mode == 2) {
-      // the tile's ReLU mask rows, coalesced, into the staging tile
-      const uint4 *src = reinterpret_cast<const uint4 *>(aux + (row * W + x0) * NOUT);
-      for (int q = tid; q < nvalid * (NOUT / 8); q += kHThreads)
-        *reinterpret_cast<uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16) = src[q];
-      __syncthreads();
-    }
-    if (half < NSPLIT) {
-      #pragma unroll
-      for (int c0 = half * CPW; c0 < (half + 1) * CPW; c0 += 16) {
-        float v[16];
-        tmem_ld16(lane_addr + c0, v);
-        if (mode == 1) {
-          if (x < W && c0 == 0) {
-            float *o = (float *)out + p * nstore;
-            if (nstore == 4) {
-              *reinterpret_cast<float4 *>(o) =
-                  make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
-            } else {
-              for (int q = 0; q < 16 && q < nstore; ++q) o[q] = v[q] + bias[q];
-            }
-          } else if (x < W) {
-            float *o = (float *)out + p * nstore;
-            for (int q = 0; q < 16; ++q)
-              if (c0 + q < nstore) o[c0 + q] = v[q] + bias[c0 + q];
+    cp_async_wait_all();
+  } else if (warp == 5) {
+    // ------------------------------------------------------------------ MMA
+    if (lane == 0) {
+      constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
+      const uint64_t adesc0 = umma_desc(Ring, kPlaneW, 128);
+      const uint64_t bdesc0 = umma_desc(Wsm, 128, KC * 128);
+      int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
+      for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
+      bool issued = false;
+      Pos a = first;
+      int it = 0;
+      for (long long tile = t0; tile < t1 && !s_stop; ++tile, ++it, a = advance(a)) {
+        const int b = it & 1;
+        bool ok = true;
+        for (int dy = -1; dy <= 1 && ok; ++dy) {
+          if (!row_used(a, dy)) continue;
+          const int r = a.gr + dy, s = r % kWsRing;
+          if (tag_row[s] == r && tag_tx[s] == a.tx) continue;
+          tag_row[s] = r;
+          tag_tx[s] = a.tx;
+          ++nload[s];
+          ok = mbar_wait(smem_u32(&full[s]), (uint32_t)((nload[s] - 1) & 1));
+        }
+        // accumulator b was last drained for tile it - 2
+        if (ok && it >= 2) ok = mbar_wait(smem_u32(&acce[b]), (uint32_t)(((it >> 1) - 1) & 1));
+        if (!ok) {
+          stop();
+          break;
+        }
+        tc_fence_after();
+        uint32_t accum = 0;
+        #pragma unroll
+        for (int tp = 0; tp < 9; ++tp) {
+          const int dy = tp / 3 - 1, dx = tp % 3 - 1;
+          if (!row_used(a, dy)) continue;
+          const int s = (a.gr + dy) % kWsRing;
+          #pragma unroll
+          for (int j = 0; j < CIN / 16; ++j) {
+            const uint64_t ad = adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kPlaneW) >> 4);
+            const uint64_t bd = bdesc0 + (uint64_t)((tp * NOUT * CIN * 2 + j * 256) >> 4);
+            umma_bf16(tmem + (uint32_t)b * NCOLS, ad, bd, idesc, accum);
+            accum = 1u;
           }
-        } else {
-          uint4 *srow = reinterpret_cast<uint4 *>(Osm + m * ROWB + c0 * 2);
-          uint32_t pk[8];
-          if (mode == 0) {
-            #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v[2 * q] + bias[c0 + 2 * q], 0.f),
-                                                              fmaxf(v[2 * q + 1] + bias[c0 + 2 * q + 1], 0.f));
-              pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
-            }
-          } else {
-            const uint4 a0 = srow[0], a1 = srow[1];
-            const uint32_t aw[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw[q]);
-              const __nv_bfloat162 b2 = __floats2bfloat162_rn(__low2float(a2) > 0.f ? v[2 * q] : 0.f,
-                                                              __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f);
-              pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
-            }
+        }
+        umma_commit(smem_u32(&accf[b]));
+        issued = true;
+        // release the rows the next tile does not read
+        if (tile + 1 < t1) {
+          const Pos n = advance(a);
+          for (int dy = -1; dy <= 1; ++dy) {
+            if (!row_used(a, dy)) continue;
+            const int r = a.gr + dy;
+            const int ndy = r - n.gr;
+            const bool kept = n.tx == a.tx && ndy >= -1 && ndy <= 1 && row_used(n, ndy);
+            if (!kept) umma_commit(smem_u32(&empty[r % kWsRing]));
           }
-          srow[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-          srow[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         }
       }
+      // every MMA issued has completed before tensor memory is freed
+      if (issued) {
+        umma_commit(smem_u32(&done));
+        if (!mbar_wait(smem_u32(&done), 0)) atomicExch(err, 1);
+      }
     }
-    if (mode != 1) {
-      __syncthreads();
-      // the tile's output rows are contiguous in global memory
-      uint4 *dst = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (row * W + x0) * NOUT);
-      for (int q = tid; q < nvalid * (NOUT / 8); q += kHThreads)
-        dst[q] = *reinterpret_cast<const uint4 *>(Osm + (q / (NOUT / 8)) * ROWB + (q % (NOUT / 8)) * 16);
+  } else {
+    // ------------------------------------------------------------- epilogue
+    const int quarter = warp;  // lane quarter of the accumulator
+    const int m = quarter * 32 + lane;
+    Pos a = first;
+    int it = 0;
+    for (long long tile = t0; tile < t1 && !s_stop; ++tile, ++it, a = advance(a)) {
+      const int b = it & 1;
+      const int x0 = a.tx * kM, x = x0 + m;
+      const long long p = (long long)a.gr * W + x;
+      // the ReLU mask of this pixel, fetched before the wait
+      uint4 am[NOUT / 8];
+      if (mode == 2) {
+        #pragma unroll
+        for (int c = 0; c < NOUT / 8; ++c)
+          am[c] = x < W ? __ldg(reinterpret_cast<const uint4 *>(aux + p * NOUT) + c) : make_uint4(0, 0, 0, 0);
+      }
+      const bool ok = mbar_wait(smem_u32(&accf[b]), (uint32_t)((it >> 1) & 1));
+      if (!ok) stop();
+      if (__any_sync(0xffffffffu, !ok)) break;
+      tc_fence_after();
+      float v[NOUT];
+      const uint32_t lane_addr = tmem + (uint32_t)b * NCOLS + ((uint32_t)(quarter * 32) << 16);
+      #pragma unroll
+      for (int c0 = 0; c0 < NOUT; c0 += 16) tmem_ld16(lane_addr + c0, v + c0);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
+      if (mode == 1) {
+        if (x < W) {
+          float *o = (float *)out + p * nstore;
+          if (nstore == 4) {
+            *reinterpret_cast<float4 *>(o) = make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
+          } else {
+            #pragma unroll
+            for (int q = 0; q < NOUT; ++q)
+              if (q < nstore) o[q] = v[q] + bias[q];
+          }
+        }
+        continue;
+      }
+      uint32_t pk[NOUT / 2];
+      #pragma unroll
+      for (int q = 0; q < NOUT / 2; ++q) {
+        float lo, hi;
+        if (mode == 0) {
+          lo = fmaxf(v[2 * q] + bias[2 * q], 0.f);
+          hi = fmaxf(v[2 * q + 1] + bias[2 * q + 1], 0.f);
+        } else {
+          const uint32_t aw = (&am[q / 4].x)[q % 4];
+          const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
+          lo = __low2float(a2) > 0.f ? v[2 * q] : 0.f;
+          hi = __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f;
+        }
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(lo, hi);
+        pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+      }
+      if (!tma) {
+        if (x < W) {
+          uint4 *o = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + p * NOUT);
+          #pragma unroll
+          for (int c = 0; c < NOUT / 8; ++c) o[c] = make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+        }
+        continue;
+      }
+      // staging tile it & 1: the store issued from it two tiles ago has read
+      // it (thread 0 issues every store, so it is the one that can tell)
+      const int sb = it & 1;
+      if (it >= 2) {
+        if (tid == 0) {
+          bulk_wait_read1();
+          mbar_arrive(smem_u32(&sfree[sb]));
+        }
+        if (!mbar_wait(smem_u32(&sfree[sb]), (uint32_t)(((it >> 1) - 1) & 1))) {
+          stop();
+          break;
+        }
+      }
+      uint8_t *row = stg_p + sb * STG + m * 128;
+      #pragma unroll
+      for (int c = 0; c < 8; ++c)  // 16-byte chunk c of the pixel's 128 bytes, 128-byte swizzle
+        *reinterpret_cast<uint4 *>(row + ((c ^ (m & 7)) << 4)) =
+            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+      fence_async_smem();
+      mbar_arrive(smem_u32(&swritten[sb]));
+      if (tid == 0) {
+        if (!mbar_wait(smem_u32(&swritten[sb]), (uint32_t)((it >> 1) & 1))) {
+          stop();
+          break;
+        }
+        tma_store3(&tmap, Stg + (uint32_t)(sb * STG), 0, x0, a.gr);
+        bulk_commit();
+      }
     }
-    tc_fence_before();
-    __syncthreads();  // accumulator b and the staging tile read before they are reused
+    if (tid == 0) bulk_wait_all();
   }
-  if (fail) {
-    // a wait gave up: record it, then wait once more (bounded) for the MMAs
-    // still in flight into this CTA's tensor memory
-    if (tid == 0) atomicExch(err, 1);
-    if (mpend) mbar_wait(smem_u32(&mbar[mpend_b]), ph[mpend_b]);
-  }
-  cp_async_wait_all();
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, 2 * NCOLS);
@@ -652,29 +709,60 @@ template <int CIN, int NOUT>
 size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 64 * 2)); }
 
 template <int CIN, int NOUT>
-size_t halo_smem() {
-  return smem_floor<NOUT>((size_t)9 * NOUT * CIN * 2 + (size_t)(CIN / 8) * kRPlane + (size_t)kM * (NOUT * 2 + 16));
+size_t ws_smem() {
+  return 1024 + (ws_tma<CIN, NOUT>() ? 2 * (size_t)kM * NOUT * 2 : 0) + (size_t)9 * NOUT * CIN * 2 +
+         (size_t)(CIN / 8) * kPlaneW;  // 64 -> 64: 1 + 32 + 72 + 97.6 KB
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry-point table (the
+// library links no libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (PFN_cuTensorMapEncodeTiled_v12000)f;
+  }();
+  return fn;
 }
 
 template <int CIN, int NOUT>
-cudaError_t conv_halo_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
-                             const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x, int mode,
-                             int nstore, int *err, cudaStream_t s) {
-  const size_t sm = halo_smem<CIN, NOUT>();
-  cudaError_t e = cudaFuncSetAttribute(k_conv_halo<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+cudaError_t conv_ws_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                           const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x, int mode,
+                           int nstore, int *err, cudaStream_t s) {
+  const size_t sm = ws_smem<CIN, NOUT>();
+  cudaError_t e = cudaFuncSetAttribute(k_conv_ws<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const long long hw = (long long)H * W;
   const int nimg = (int)(npix / hw);
-  const long long ntiles = (long long)nimg * H * ((W + kM - 1) / kM);
+  const long long NR = (long long)nimg * H;
+  const long long ntiles = NR * ((W + kM - 1) / kM);
+  // output tensor map: [image rows][W][NOUT] BF16, box = one tile (128 pixels
+  // x 64 channels), 128-byte swizzle; pixels past W in a tile are not stored
+  CUtensorMap tm;
+  memset(&tm, 0, sizeof tm);
+  if (ws_tma<CIN, NOUT>() && mode != 1) {
+    auto enc = tensor_map_encoder();
+    if (!enc || NR > 0x7fffffffLL || ((uintptr_t)out & 15u)) return cudaErrorInvalidValue;
+    const cuuint64_t dims[3] = {(cuuint64_t)NOUT, (cuuint64_t)W, (cuuint64_t)NR};
+    const cuuint64_t strides[2] = {(cuuint64_t)NOUT * 2, (cuuint64_t)W * NOUT * 2};
+    const cuuint32_t box[3] = {(cuuint32_t)NOUT, (cuuint32_t)kM, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, out, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+  }
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_halo<CIN, NOUT>, kHThreads, sm);
-  const int tmem_cap = 512 / (2 * (NOUT < 32 ? 32 : NOUT));  // two accumulators per CTA
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_ws<CIN, NOUT>, kWsThreads, sm);
+  const int tmem_cap = 512 / (2 * (NOUT < 32 ? 32 : NOUT));
   per = per < 1 ? 1 : (per > tmem_cap ? tmem_cap : per);
   const long long grid = ntiles < (long long)nsm * per ? ntiles : (long long)nsm * per;
-  k_conv_halo<CIN, NOUT><<<(unsigned)grid, kHThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
-                                                               nstore, err);
+  k_conv_ws<CIN, NOUT><<<(unsigned)grid, kWsThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
+                                                               nstore, err, tm);
   return cudaGetLastError();
 }
 
@@ -682,9 +770,9 @@ template <int CIN, int NOUT>
 cudaError_t conv_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, const __nv_bfloat16 *aux,
                         void *out, long long npix, int H, int W, int periodic_x, int mode, int nstore, int *err,
                         cudaStream_t s) {
-  // whole images: the persistent halo form
+  // whole images: the persistent warp-specialised form
   if (npix % ((long long)H * W) == 0)
-    return conv_halo_launch<CIN, NOUT>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+    return conv_ws_launch<CIN, NOUT>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
   const size_t sm = conv_smem<CIN, NOUT>();
   cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
