@@ -365,7 +365,10 @@ def run_ours(args):
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": round(achieved, 1),
                          "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-                         "algorithmic_bytes_per_launch": kbytes},
+                         "algorithmic_bytes_per_launch": kbytes,
+                         # the barotropic subcycle keeps its state on chip: its
+                         # time is the latency of 120 dependent substeps
+                         "us_per_substep": round(avg_s * 1e6 / nstep, 3) if kname == "int_trop" else None},
             "kernels": kernels,
             "gpu_launches": int(launches),
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
