@@ -85,7 +85,6 @@ def parse():
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     p.add_argument("--no-closure", action="store_true", help="skip the closure-network leg")
     p.add_argument("--no-global025", action="store_true", help="skip the 0.25-degree leg")
-    p.add_argument("--no-fma", action="store_true", help="skip the FMA-contracted legs")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     p.add_argument("--decomp", action="store_true",
                    help="one 1-degree domain split into row slabs over the N ranks (strong scaling) "
@@ -119,6 +118,10 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: begin timing once it samples
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -224,8 +227,10 @@ def run_ours(args):
 
     launches0 = m.launch_count()
     barrier()
-    with Clocks(dev) as clk:
-        t_ms = device_loop(it0 + 1)
+    # clocks are sampled over every timed loop below (device-resident, with
+    # kernel events, end to end): the first alone is ~60 ms
+    clk = Clocks(dev).__enter__()
+    t_ms = device_loop(it0 + 1)
     launches = m.launch_count() - launches0
     L.check(lib.pcom_gpu_check_finite(h), "watchdog")
     t_max = max_over_ranks(t_ms, world, "cuda")
@@ -288,6 +293,7 @@ def run_ours(args):
     e2e_ms = e2e_loop(it1 + 1, True)
     e2e = replica_sypd(e2e_ms / steps, world)
     e2e_sync = replica_sypd(e2e_loop(it1 + 1 + steps, False) / steps, world)
+    clk.__exit__(None, None, None)
 
     # ------------------------------------------------ roofline of the dominant kernel
     peaks = {}
@@ -318,11 +324,6 @@ def run_ours(args):
     mixed = None
     if not args.no_mixed:
         mixed = run_mixed_leg(args, case, stream, steps)
-    # the FP64 path with the FMA-contracted kernels (PCOM_FMA) and the mixed
-    # path with them
-    fma = None
-    if not args.no_fma:
-        fma = run_fma_leg(args, case, stream, steps)
     closure = None
     if not args.no_closure:
         closure = run_closure_leg(args, case, ms_per_step)
@@ -374,7 +375,6 @@ def run_ours(args):
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "cpu_baseline": cpu,
             "mixed": mixed,
-            "fma": fma,
             "closure": closure,
             "global025": global025,
             "ensemble": ensemble,
@@ -427,61 +427,6 @@ def run_mixed_leg(args, case, stream, steps):
     b.close()
     return {"ms_per_step": round(ms, 4), "value": round(sypd(ms / 1000.0), 2), "unit": "SYPD", "dtype": "f32 stencils and barotropic velocities, f64 bottom pressure",
             "rel_rms_error_vs_fp64_after_24_steps": {k_: float(f"{v:.3e}") for k_, v in err.items()}}
-
-
-def device_ms_per_step(m, stream, steps: int, warmup: int) -> float:
-    """CUDA-event time per step of `steps` device-resident steps (den_prho on
-    day change) after `warmup` steps through the host driver."""
-    import torch
-
-    from pcom_b200 import _lib as L
-
-    m.set_stream(stream.cuda_stream)
-    m.run(max(warmup, 3))
-    it0 = m.iter
-    day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for q in range(steps):
-        it = it0 + 1 + q
-        if day_of(it) != day_of(it - 1):
-            L.check(m.lib.pcom_gpu_den_prho(m.handle), "den_prho")
-        L.check(m.lib.pcom_gpu_step_async(m.handle, it), "step")
-    e1.record(stream)
-    torch.cuda.synchronize()
-    m.check_finite()
-    return e0.elapsed_time(e1) / steps
-
-
-def run_fma_leg(args, case, stream, steps):
-    """PCOM_FMA handles: the FP64 path and the mixed path with the step
-    kernels built with FMA contraction, and the FP64 FMA path's largest
-    relative difference from the exact FP64 path after 1 and 24 steps."""
-    from pcom_b200 import _lib as L
-    from pcom_b200.model import Model
-
-    out = {}
-    for name, flags in (("fp64", L.PCOM_FMA), ("mixed", L.PCOM_PREC_MIXED | L.PCOM_FMA)):
-        m = Model(case, flags=flags)
-        ms = device_ms_per_step(m, stream, steps, args.warmup)
-        m.close()
-        out[name] = {"ms_per_step": round(ms, 4), "value": round(sypd(ms / 1000.0), 2), "unit": "SYPD"}
-    a, b = Model(case), Model(case, flags=L.PCOM_FMA)
-    diff = {}
-    for n in (1, 24):
-        a.run(n - a.iter)
-        b.run(n - b.iter)
-        worst = 0.0
-        for f in ("tc", "sc", "uc", "vc", "chc", "ubc", "vbc", "wm", "am"):
-            x, y = b.field(f), a.field(f)
-            worst = max(worst, float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300)))
-        diff[f"after_{n}_steps"] = float(f"{worst:.3e}")
-    a.close()
-    b.close()
-    out["fp64"]["max_rel_diff_vs_exact_fp64"] = diff
-    return out
 
 
 def run_closure_leg(args, case, plain_ms):

@@ -14,7 +14,7 @@ module mod_pcom_gpu
 
   integer(c_int), parameter :: PCOM_OK = 0, PCOM_ERR_ARG = 1, PCOM_ERR_CUDA = 2, &
                                PCOM_ERR_STATE = 3, PCOM_ERR_NUMERIC = 4, PCOM_ERR_TIMEOUT = 5
-  integer(c_int32_t), parameter :: PCOM_PREC_FP64 = 0, PCOM_PREC_MIXED = 1, PCOM_FMA = 2, PCOM_LIT_R8 = 16
+  integer(c_int32_t), parameter :: PCOM_PREC_FP64 = 0, PCOM_PREC_MIXED = 1, PCOM_LIT_R8 = 16
 
   ! sizes and time steps (mod_param.f90:40-81)
   type, bind(c) :: pcom_dims

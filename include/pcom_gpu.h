@@ -51,13 +51,6 @@ extern "C" {
 #define PCOM_PREC_MIXED 0x1
 #define PCOM_LIT_R8 0x10     /* default-REAL literals read as REAL(8) (ifort -r8);
                                 otherwise REAL(4) as gfortran compiles them */
-/* FMA: the step kernels built with a*b+c contracted into fused multiply-adds
- * (one rounding instead of two).  Without it every operation rounds where the
- * reference's x86-64 build (gfortran -O2, no contraction) rounds, and the FP64
- * path is bit-equal to it; with it the FP64 fields stay within 1e-12 relative
- * of that after one step, and the step is shorter.  Applies to either
- * precision.  No counterpart in the reference. */
-#define PCOM_FMA 0x2
 
 typedef struct pcom_handle pcom_handle;
 
@@ -67,7 +60,7 @@ typedef struct pcom_dims {
   int32_t glo_ni, glo_nj, nk;
   int32_t ni, nj;          /* must equal glo_ni + 2, glo_nj + 2 */
   int32_t dtbt, dtbc;      /* barotropic / baroclinic step (s) */
-  int32_t flags;           /* PCOM_PREC_* | PCOM_FMA | PCOM_LIT_R8 */
+  int32_t flags;           /* PCOM_PREC_* | PCOM_LIT_R8 */
   int32_t rst;             /* nm%rst: 1 = restart run (skips the AB3 start-up) */
   int32_t reserved[3];
 } pcom_dims;

@@ -42,7 +42,7 @@ typedef struct pcom_model pcom_model;
 #define PCOM_MODEL_HOST_ONLY 0x100
 
 /* Setup (main.f90:86-150) and the GPU handle with static data and initial
- * state uploaded.  flags: PCOM_PREC_* | PCOM_FMA (PCOM_LIT_R8 is taken from case->r8). */
+ * state uploaded.  flags: PCOM_PREC_* (PCOM_LIT_R8 is taken from case->r8). */
 int pcom_model_create(const pcom_case *c, int32_t flags, pcom_model **out);
 int pcom_model_destroy(pcom_model *m);
 pcom_handle *pcom_model_handle(pcom_model *m);

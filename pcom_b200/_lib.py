@@ -17,7 +17,6 @@ PCOM_OK = 0
 ERRORS = {1: "PCOM_ERR_ARG", 2: "PCOM_ERR_CUDA", 3: "PCOM_ERR_STATE", 4: "PCOM_ERR_NUMERIC", 5: "PCOM_ERR_TIMEOUT"}
 PCOM_PREC_FP64 = 0x0
 PCOM_PREC_MIXED = 0x1
-PCOM_FMA = 0x2
 PCOM_LIT_R8 = 0x10
 PCOM_MODEL_HOST_ONLY = 0x100
 

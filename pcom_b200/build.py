@@ -1,11 +1,8 @@
 """Build libpcomgpu.so in-tree for sm_100a with nvcc.
 
-The step kernels (k_step.cu, k_trop.cu, k_trop_batch.cu) are compiled twice:
-with ``--fmad=false`` (no FMA contraction) into namespace ``kx_exact``, so
-that every operation rounds exactly where the reference's x86-64 build
-rounds, and with ``--fmad=true`` into namespace ``kx_fma`` for handles created
-with PCOM_FMA.  The host driver is compiled with ``-ffp-contract=off``.
-Objects are compiled in parallel.
+The FP64 kernels are compiled with ``--fmad=false`` (no FMA contraction) so
+that every operation rounds exactly where the reference's x86-64 build rounds;
+the host driver is compiled with ``-ffp-contract=off`` for the same reason.
 """
 from __future__ import annotations
 
@@ -20,11 +17,9 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpcomgpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_VARIANT = ["k_step.cu", "k_trop.cu", "k_trop_batch.cu"]  # built exact and contracted
-CU_FP64 = ["pcom_gpu.cu", "k_trop_noalloc.cu"]
+CU_FP64 = ["k_step.cu", "k_trop.cu", "pcom_gpu.cu", "k_trop_noalloc.cu", "k_trop_batch.cu"]
 CU_FAST = ["k_cnn.cu", "cnn.cu", "k_trop_mixed.cu"]  # may contract a*b+c into FMA: closure network, mixed barotropic
 CPP = ["pcom_host.cpp"]
-VARIANTS = {"exact": ["--fmad=false", "-DPCOM_KNS=kx_exact"], "fma": ["--fmad=true", "-DPCOM_KNS=kx_fma"]}
 
 
 def _nvcc() -> str:
@@ -40,8 +35,8 @@ def _host_cxx() -> str:
 
 
 def _sources():
-    return [os.path.join(SRC, f) for f in CU_VARIANT + CU_FP64 + CU_FAST + CPP] + [
-        os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".cuh", ".h", ".inc"))
+    return [os.path.join(SRC, f) for f in CU_FP64 + CU_FAST + CPP] + [
+        os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".cuh", ".h"))
     ] + [os.path.join(HERE, "..", "include", f) for f in ("pcom_gpu.h", "pcom_host.h", "pcom_cnn.h")]
 
 
@@ -61,30 +56,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = _nvcc()
     cxx = _host_cxx()
     common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", cxx]
-    jobs = []  # (command, object)
-    for f in CU_VARIANT:
-        for v, flags in VARIANTS.items():
-            o = os.path.join(obj_dir, f"{f}.{v}.o")
-            jobs.append(([nvcc, *ARCH, *common, *flags, "-c", os.path.join(SRC, f), "-o", o], o))
+    objs = []
     for f in CU_FP64 + CU_FAST:
         o = os.path.join(obj_dir, f + ".o")
         fmad = ["--fmad=false"] if f in CU_FP64 else ["--fmad=true"]
-        jobs.append(([nvcc, *ARCH, *common, *fmad, "-c", os.path.join(SRC, f), "-o", o], o))
+        cmd = [nvcc, *ARCH, *common, *fmad, "-c", os.path.join(SRC, f), "-o", o]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(o)
     for f in CPP:
         o = os.path.join(obj_dir, f + ".o")
-        jobs.append(([cxx, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-c", os.path.join(SRC, f), "-o", o], o))
-    if verbose:
-        for cmd, _ in jobs:
+        cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-c", os.path.join(SRC, f), "-o", o]
+        if verbose:
             print(" ".join(cmd))
-    from concurrent.futures import ThreadPoolExecutor
-
-    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
-        results = list(ex.map(lambda j: subprocess.run(j[0], capture_output=True, text=True), jobs))
-    for (cmd, _), r in zip(jobs, results):
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise subprocess.CalledProcessError(r.returncode, cmd)
-    objs = [o for _, o in jobs]
+        subprocess.run(cmd, check=True)
+        objs.append(o)
     cmd = [nvcc, *ARCH, "-shared", "-ccbin", cxx, "-cudart", "static", "-o", LIB, *objs,
            "-Xlinker", "--exclude-libs,ALL"]
     if verbose:

@@ -262,8 +262,7 @@ VARIANTS = {  # applied fraction of each output (du, dv, dT, dS) and the |y| cli
 # state fields pcom_gpu_coarsen sets (what a coarse run starts from)
 START_FIELDS = ("tc", "sc", "tp", "sp", "uc", "vc", "up", "vp", "auc", "aup", "aupp", "avc", "avp", "avpp",
                 "ubc", "vbc", "ubp", "vbp", "chc", "chp", "mch", "mch2", "am")
-FLAGS = {"fp64": L.PCOM_PREC_FP64, "fp64-fma": L.PCOM_FMA, "mixed": L.PCOM_PREC_MIXED,
-         "mixed-fma": L.PCOM_PREC_MIXED | L.PCOM_FMA}
+FLAGS = {"fp64": L.PCOM_PREC_FP64, "mixed": L.PCOM_PREC_MIXED}
 
 
 def coarse_run(exp: Experiment, flags: int) -> Model:

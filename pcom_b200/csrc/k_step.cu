@@ -22,9 +22,6 @@
 #include "pcom_dev.cuh"
 #include "pcom_kernels.h"
 
-// compiled twice: PCOM_KNS is kx_exact (no FMA contraction) or kx_fma
-namespace PCOM_KNS {
-
 // block of the level-parallel 3-D kernels: 32 columns of one row x TB_K
 // threads down the levels.  8 (256 threads) rather than 16: the kernels
 // end in a serial column pass by one or two warps, and smaller blocks let
@@ -1384,5 +1381,3 @@ void launch_batch(int kernel, const Dev *dPs, const BatchShape &b, int arg, cuda
   default: break;
   }
 }
-
-}  // namespace PCOM_KNS

@@ -20,9 +20,6 @@
 #include "pcom_dev.cuh"
 #include "pcom_kernels.h"
 
-// compiled twice: PCOM_KNS is kx_exact (no FMA contraction) or kx_fma
-namespace PCOM_KNS {
-
 namespace {
 
 constexpr long long kSpinLimit = 1LL << 26;  // ~seconds with the nanosleep below
@@ -1062,5 +1059,3 @@ cudaError_t launch_trop_group(const Dev *dPs, const TileRef *dtiles, int ntiles,
                   (void *)&cnt, (void *)&err};
   return cudaLaunchCooperativeKernel(fn, dim3(ntiles), dim3(nthreads), args, smem, s);
 }
-
-}  // namespace PCOM_KNS

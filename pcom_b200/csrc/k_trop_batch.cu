@@ -16,9 +16,6 @@
 #include "pcom_dev.cuh"
 #include "pcom_kernels.h"
 
-// compiled twice: PCOM_KNS is kx_exact (no FMA contraction) or kx_fma
-namespace PCOM_KNS {
-
 namespace {
 
 
@@ -369,5 +366,3 @@ cudaError_t launch_trop_multi(const Dev &P, const TileRef *dtiles, int ntiles, i
   return launch_batch_form(batch_kernel<true>(TX, TY), batch_threads<true>(), P, nullptr, dtiles, ntiles, TX, TY,
                            nblocks, cnt, err, s);
 }
-
-}  // namespace PCOM_KNS

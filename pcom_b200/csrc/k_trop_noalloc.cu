@@ -158,17 +158,17 @@ extern "C" int pcom_gpu_trop_noalloc(const pcom_trop_io *io, void *stream_) {
 
   // tiling: the resident kernel with the fewest tiles that are co-resident
   int bx = 0, by = 0, best = 1 << 30;
-  const int mb = kx_exact::trop_res_max_blocks(24, 18);
+  const int mb = trop_res_max_blocks(24, 18);
   for (int ty = 6; ty <= 40; ++ty)
     for (int tx = 6; tx <= 60; ++tx) {
-      if (!kx_exact::trop_res_fits(tx, ty)) continue;
+      if (!trop_res_fits(tx, ty)) continue;
       const int nt = ((io->glo_ni + tx - 1) / tx) * ((nj + ty - 1) / ty);
       if (nt > mb) continue;
       if (nt < best || (nt == best && (tx + 4) * (ty + 4) < (bx + 4) * (by + 4))) { best = nt; bx = tx; by = ty; }
     }
-  if (bx == 0 || kx_exact::trop_res_max_blocks(bx, by) < best)
+  if (bx == 0 || trop_res_max_blocks(bx, by) < best)
     return error(PCOM_ERR_ARG, "pcom_gpu_trop_noalloc: the domain does not fit one co-resident tile per CTA");
-  if (kx_exact::launch_trop_res(D, bx, by, s) != cudaSuccess)
+  if (launch_trop_res(D, bx, by, s) != cudaSuccess)
     return error(PCOM_ERR_CUDA, "pcom_gpu_trop_noalloc: kernel launch failed");
   int flags[2] = {0, 0};
   if (cudaMemcpyAsync(flags, D.err, sizeof flags, cudaMemcpyDeviceToHost, s) != cudaSuccess ||

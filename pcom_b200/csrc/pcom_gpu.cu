@@ -323,9 +323,6 @@ void launch_nonfinite(const double *f, const int *lev, int nk, long long n2, int
   k_nonfinite<double><<<592, 256, 0, s>>>(f, lev, nk, n2, planes, count);
 }
 
-// the launcher namespace of the handle's build (exact or FMA-contracted)
-#define KFN(obj, name) ((obj)->fma ? &kx_fma::name : &kx_exact::name)
-
 struct pcom_handle {
   pcom_dims dims{};
   int ni = 0, nj = 0, nk = 0, nkp = 0;
@@ -337,7 +334,6 @@ struct pcom_handle {
   // mixed path: the 3-D fields live in DM (FP32); D keeps the shared FP64
   // part and serves the barotropic kernel (its am is the FP64 level-1 copy)
   bool mixed = false;
-  bool fma = false;  // PCOM_FMA: the contracted build of the step kernels
   DevM DM{};
   float *ab_uf[3] = {}, *ab_vf[3] = {}, *t_poolf[3] = {}, *s_poolf[3] = {};
   double *stage = nullptr;     // FP64 staging for host copies of FP32 fields
@@ -487,15 +483,15 @@ int pick_trop_config(pcom_handle *h) {
   h->trop_multi = false;
   if (h->D.separable && (h->trop_force == 0 || h->trop_force == 1)) {
     int best_n = 1 << 30, bx = 0, by = 0;
-    const int mb = KFN(h, trop_fast_max_blocks)(24, 18);
+    const int mb = trop_fast_max_blocks(24, 18);
     for (int ty = 6; ty <= 40; ++ty)
       for (int tx = 6; tx <= 60; ++tx) {
-        if (!KFN(h, trop_res_fits)(tx, ty)) continue;
+        if (!trop_res_fits(tx, ty)) continue;
         const int nt = ((h->dims.glo_ni + tx - 1) / tx) * ((h->nj + ty - 1) / ty);
         if (nt > mb) continue;
         if (nt < best_n || (nt == best_n && (tx + 4) * (ty + 4) < (bx + 4) * (by + 4))) { best_n = nt; bx = tx; by = ty; }
       }
-    if (bx > 0 && KFN(h, trop_fast_max_blocks)(bx, by) >= best_n) {
+    if (bx > 0 && trop_fast_max_blocks(bx, by) >= best_n) {
       h->trop_resident = true;
       h->trop_tx = bx;
       h->trop_ty = by;
@@ -508,7 +504,7 @@ int pick_trop_config(pcom_handle *h) {
   if (h->trop_force == 1) return fail(PCOM_ERR_ARG, "the domain does not fit the resident barotropic kernel");
   if (h->D.separable && (h->trop_force == 0 || h->trop_force == 2)) {
     const int tx = 32, ty = 10;
-    const int mb = KFN(h, trop_batch_max_blocks)(tx, ty);
+    const int mb = trop_batch_max_blocks(tx, ty);
     if (mb > 0) {
       std::vector<TileRef> t;
       const int G = h->dims.glo_ni, nj = h->nj;
@@ -535,7 +531,7 @@ int pick_trop_config(pcom_handle *h) {
   for (auto &c : cand) {
     const int tx = c[0], ty = c[1];
     const int nt = ((h->dims.glo_ni + tx - 1) / tx) * ((h->nj + ty - 1) / ty);
-    const int mb = KFN(h, trop_max_blocks)(tx, ty);
+    const int mb = trop_max_blocks(tx, ty);
     if (mb <= 0) continue;
     h->trop_tx = tx;
     h->trop_ty = ty;
@@ -547,23 +543,15 @@ int pick_trop_config(pcom_handle *h) {
 }
 
 // ---- the pieces of the step (FP64 handle: D; mixed handle: DM)
-#define ON_DEV_PREC(call_on) \
-  if (h->mixed) {            \
-    auto &X = h->DM;         \
-    call_on;                 \
-  } else {                   \
-    auto &X = h->D;          \
-    call_on;                 \
-  }
-#define ON_DEV(call_on)              \
-  do {                               \
-    if (h->fma) {                    \
-      using namespace kx_fma;        \
-      ON_DEV_PREC(call_on)           \
-    } else {                         \
-      using namespace kx_exact;      \
-      ON_DEV_PREC(call_on)           \
-    }                                \
+#define ON_DEV(call_on) \
+  do {                  \
+    if (h->mixed) {     \
+      auto &X = h->DM;  \
+      call_on;          \
+    } else {            \
+      auto &X = h->D;   \
+      call_on;          \
+    }                   \
   } while (0)
 int do_den_alpha(pcom_handle *h) {
   Prof p(h, "den_alpha+int_tobot");
@@ -626,13 +614,13 @@ int do_trop(pcom_handle *h) {
     if (h->mixed && trop_mixed_max_blocks(h->trop_tx, h->trop_ty) >= h->trop_blocks)
       e = launch_trop_mixed(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     else
-      e = KFN(h, launch_trop_fast)(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
+      e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
   } else if (h->trop_multi) {
-    e = KFN(h, launch_trop_multi)(h->D, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1, h->D.err,
+    e = launch_trop_multi(h->D, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1, h->D.err,
                           h->stream);
   } else {
-    e = KFN(h, launch_trop)(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
+    e = launch_trop(h->D, h->trop_tx, h->trop_ty, h->trop_blocks, h->stream);
   }
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "barotropic kernel launch: %s", cudaGetErrorString(e));
   h->n_ch++;
@@ -983,7 +971,6 @@ int pcom_gpu_create(const pcom_dims *dims, pcom_handle **out) {
   if (d.dtbt <= 0 || d.dtbc <= 0 || d.dtbc % d.dtbt != 0) return fail(PCOM_ERR_ARG, "dtbc must be a positive multiple of dtbt");
   pcom_handle *h = new pcom_handle();
   h->mixed = (d.flags & PCOM_PREC_MIXED) != 0;
-  h->fma = (d.flags & PCOM_FMA) != 0;
   h->dims = d;
   h->ni = d.ni; h->nj = d.nj; h->nk = d.nk; h->nkp = d.nk + 1;
   h->n2 = (long long)d.ni * d.nj;
@@ -1428,7 +1415,8 @@ int pcom_gpu_den_prho(pcom_handle *h) {
   if (!h->static_ok) return fail(PCOM_ERR_STATE, "den_prho before pcom_gpu_upload_static");
   {
     Prof p(h, "den_prho");
-    ON_DEV(launch_den_prho(X, h->stream));
+    if (h->mixed) launch_den_prho(h->DM, h->stream);
+    else launch_den_prho(h->D, h->stream);
   }
   return sync_check(h);
 }
@@ -1727,7 +1715,6 @@ int pcom_set_error(int code, const char *msg) { return fail(code, "%s", msg); }
 // whole step can be captured into CUDA graphs (one per ring-buffer phase).
 struct pcom_batch {
   std::vector<pcom_handle *> hs;
-  bool fma = false;  // the members' build of the step kernels (all members alike)
   // the batch's own stream (capturable), joined by events to the members'
   // streams before and after its work
   cudaStream_t stream = nullptr;
@@ -1784,7 +1771,7 @@ int batch_tiles(pcom_batch *b, int TX, int TY) {
   b->groups.clear();
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  int cap = KFN(b, trop_group_max_blocks)(TX, TY);
+  int cap = trop_group_max_blocks(TX, TY);
   if (b->max_resident > 0) cap = std::min(cap, b->max_resident);
   const int n = (int)b->hs.size();
   std::vector<std::vector<TileRef>> mt(n);
@@ -1817,7 +1804,7 @@ int batch_tiles(pcom_batch *b, int TX, int TY) {
     if (resident) {
       g.nblocks = g.ntiles;
     } else {
-      const int mb = KFN(b, trop_batch_max_blocks)(TX, TY);
+      const int mb = trop_batch_max_blocks(TX, TY);
       if (mb <= 0) return fail(PCOM_ERR_ARG, "tile %dx%d does not fit the multi-tile barotropic kernel", TX, TY);
       g.nblocks = std::min(g.ntiles, mb);
     }
@@ -1840,9 +1827,8 @@ int batch_tiles(pcom_batch *b, int TX, int TY) {
 // the barotropic subcycles of all members
 cudaError_t batch_trop(pcom_batch *b, const Dev *dP) {
   for (const pcom_batch::TropGroup &g : b->groups) {
-    cudaError_t e = g.resident ? KFN(b, launch_trop_group)(dP, g.d, g.ntiles, b->TX, b->TY, b->cnt, b->err, b->stream)
-                               : KFN(b, launch_trop_batch)(dP, g.d, g.ntiles, b->TX, b->TY, g.nblocks, b->cnt, b->err,
-                                                           b->stream);
+    cudaError_t e = g.resident ? launch_trop_group(dP, g.d, g.ntiles, b->TX, b->TY, b->cnt, b->err, b->stream)
+                               : launch_trop_batch(dP, g.d, g.ntiles, b->TX, b->TY, g.nblocks, b->cnt, b->err, b->stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1892,20 +1878,20 @@ int batch_dev_array(pcom_batch *b, int key, Dev **out) {
 int batch_enqueue(pcom_batch *b, Dev *dP) {
   const BatchShape &s = b->shape;
   cudaStream_t st = b->stream;
-  KFN(b, launch_batch)(BK_ALPHA_TOBOT, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_PGRA2D, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_UV2D, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_UPWELLING, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_READYC3D, dP, s, 0, st);
+  launch_batch(BK_ALPHA_TOBOT, dP, s, 0, st);
+  launch_batch(BK_PGRA2D, dP, s, 0, st);
+  launch_batch(BK_UV2D, dP, s, 0, st);
+  launch_batch(BK_UPWELLING, dP, s, 0, st);
+  launch_batch(BK_READYC3D, dP, s, 0, st);
   cudaError_t e = batch_trop(b, dP);
   if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "batched barotropic launch: %s", cudaGetErrorString(e));
-  KFN(b, launch_batch)(BK_UV2D, dP, s, 2, st);
-  KFN(b, launch_batch)(BK_CLIN, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_SMAG, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_SSH, dP, s, 0, st);
-  KFN(b, launch_batch)(BK_UV2D, dP, s, 1, st);
-  KFN(b, launch_batch)(BK_UPWELLING, dP, s, 1, st);
-  KFN(b, launch_batch)(BK_TS, dP, s, 0, st);
+  launch_batch(BK_UV2D, dP, s, 2, st);
+  launch_batch(BK_CLIN, dP, s, 0, st);
+  launch_batch(BK_SMAG, dP, s, 0, st);
+  launch_batch(BK_SSH, dP, s, 0, st);
+  launch_batch(BK_UV2D, dP, s, 1, st);
+  launch_batch(BK_UPWELLING, dP, s, 1, st);
+  launch_batch(BK_TS, dP, s, 0, st);
   CK(cudaGetLastError());
   return PCOM_OK;
 }
@@ -1930,13 +1916,11 @@ extern "C" {
 int pcom_gpu_batch_create(pcom_handle *const *hs, int32_t n, pcom_batch **out) {
   if (!hs || n <= 0 || !out) return fail(PCOM_ERR_ARG, "null argument or empty batch");
   pcom_batch *b = new pcom_batch();
-  b->fma = hs[0] && hs[0]->fma;
   for (int m = 0; m < n; ++m) {
     pcom_handle *h = hs[m];
     if (!h || !h->static_ok) { delete b; return fail(PCOM_ERR_STATE, "batch member %d has no static data", m); }
     if (!h->D.separable) { delete b; return fail(PCOM_ERR_ARG, "batch member %d: batches need lat-lon (separable) metrics", m); }
     if (h->mixed) { delete b; return fail(PCOM_ERR_ARG, "batch member %d: batches run the FP64 path only", m); }
-    if (h->fma != hs[0]->fma) { delete b; return fail(PCOM_ERR_ARG, "batch members must share the PCOM_FMA flag"); }
     if (h->D.bt != hs[0]->D.bt || h->D.bc != hs[0]->D.bc) { delete b; return fail(PCOM_ERR_ARG, "batch members must share dtbt and dtbc"); }
     if (h->device != hs[0]->device) { delete b; return fail(PCOM_ERR_ARG, "batch members must live on one device"); }
     b->hs.push_back(h);
@@ -1984,7 +1968,7 @@ int pcom_gpu_batch_den_prho(pcom_batch *b) {
   rc = batch_dev_array(b, phase_key(b->hs[0]), &dP);
   if (rc) return rc;
   b->launches++;
-  KFN(b, launch_batch)(BK_DEN_PRHO, dP, b->shape, 0, b->stream);
+  launch_batch(BK_DEN_PRHO, dP, b->shape, 0, b->stream);
   rc = batch_join_out(b);
   if (rc) return rc;
   return batch_sync(b);
@@ -2136,7 +2120,7 @@ int pcom_gpu_batch_autotune(pcom_batch *b, char *report, int32_t len) {
   cudaEventCreate(&e1);
   for (auto &c : cand) {
     if (rc) break;
-    if (KFN(b, trop_group_max_blocks)(c[0], c[1]) <= 0) continue;
+    if (trop_group_max_blocks(c[0], c[1]) <= 0) continue;
     rc = batch_tiles(b, c[0], c[1]);
     if (rc) break;
     float ms = 0.f, tot = 0.f;

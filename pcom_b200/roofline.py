@@ -81,12 +81,12 @@ def _steps(m, first: int, n: int, day_of):
         L.check(lib.pcom_gpu_step_async(m.handle, it), "step")
 
 
-def kernel_table(case: dict, mixed: bool, steps: int, fma: bool = False) -> dict:
+def kernel_table(case: dict, mixed: bool, steps: int) -> dict:
     import torch
 
     from .model import Model
 
-    m = Model(case, flags=(L.PCOM_PREC_MIXED if mixed else L.PCOM_PREC_FP64) | (L.PCOM_FMA if fma else 0))
+    m = Model(case, flags=L.PCOM_PREC_MIXED if mixed else L.PCOM_PREC_FP64)
     m.run(3)  # AB3 start-up and a warm cache of kernels
     spd = 86400 // case["dtbc"]
     day_of = lambda it: (it - 1) // spd
@@ -217,13 +217,12 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=12, help="steps timed per path (and again with events)")
     ap.add_argument("--days", type=float, default=0.0, help="model days of the time loop on both paths")
     ap.add_argument("--json", default=None)
-    ap.add_argument("--fma", action="store_true", help="the PCOM_FMA builds of the step kernels")
     ap.add_argument("--cnn", type=int, default=0, help="also time N forward passes and training steps of the "
                                                       "closure network on the case's level images")
     a = ap.parse_args(argv)
     case = make_case(a.case)
     rep = {"case": a.case, "grid": [case["glo_ni"], case["glo_nj"], case["nk"]], "steps": a.steps,
-           "fp64": kernel_table(case, False, a.steps, a.fma), "mixed": kernel_table(case, True, a.steps, a.fma)}
+           "fp64": kernel_table(case, False, a.steps), "mixed": kernel_table(case, True, a.steps)}
     if a.days > 0:
         rep["days_run"] = days_run(case, a.days)
     if a.cnn > 0:
