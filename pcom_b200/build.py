@@ -18,7 +18,8 @@ LIB = os.path.join(OUT_DIR, "libpcomgpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FP64 = ["k_step.cu", "k_trop.cu", "pcom_gpu.cu", "k_trop_noalloc.cu", "k_trop_batch.cu"]
-CU_FAST = ["k_cnn.cu", "cnn.cu", "k_trop_mixed.cu"]  # may contract a*b+c into FMA: closure network, mixed barotropic
+# may contract a*b+c into FMA: closure network, mixed barotropic kernels
+CU_FAST = ["k_cnn.cu", "cnn.cu", "k_trop_mixed.cu", "k_trop_multi_mixed.cu"]
 CPP = ["pcom_host.cpp"]
 
 

@@ -353,6 +353,9 @@ struct pcom_handle {
   // domains too large for the resident kernel: the multi-tile kernel over
   // this domain's tile list (its Dev passed by value per launch)
   bool trop_multi = false;
+  // mixed handles on the multi-tile path: FP32 coefficients and velocities
+  unsigned char *mm_scratch = nullptr;
+  MultiMixed mm{};
   int trop_force = 0;  // 0 automatic, 1 resident, 2 multi-tile, 3 generic
   TileRef *d_tiles1 = nullptr;
   int ntiles1 = 0;
@@ -522,6 +525,16 @@ int pick_trop_config(pcom_handle *h) {
       h->trop_tx = tx;
       h->trop_ty = ty;
       h->trop_blocks = std::min(h->ntiles1, mb);
+      if (h->mixed) {
+        const int mmb = trop_multi_mixed_max_blocks(tx, ty);
+        if (mmb <= 0) return fail(PCOM_ERR_CUDA, "the mixed multi-tile barotropic kernel cannot be launched");
+        if (!h->mm_scratch) {
+          rc = h->alloc(&h->mm_scratch, trop_multi_mixed_scratch_bytes(h->n2));
+          if (rc) return rc;
+          trop_multi_mixed_bind(h->mm, h->mm_scratch, h->n2);
+        }
+        h->trop_blocks = std::min(h->ntiles1, mmb);
+      }
       return PCOM_OK;
     }
   }
@@ -616,6 +629,9 @@ int do_trop(pcom_handle *h) {
     else
       e = launch_trop_fast(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
     h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
+  } else if (h->trop_multi && h->mixed) {
+    e = launch_trop_multi_mixed(h->D, h->mm, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks,
+                                h->d_cnt1, h->D.err, h->stream);
   } else if (h->trop_multi) {
     e = launch_trop_multi(h->D, h->d_tiles1, h->ntiles1, h->trop_tx, h->trop_ty, h->trop_blocks, h->d_cnt1, h->D.err,
                           h->stream);

@@ -49,11 +49,28 @@ int trop_fast_max_blocks(int TX, int TY);
 // mixed path: the resident kernel with FP32 arithmetic outside the bottom pressure
 cudaError_t launch_trop_mixed(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
 int trop_mixed_max_blocks(int TX, int TY);
-
 // batched barotropic subcycle: one persistent launch over the tiles of all members
 struct TileRef {
   int m, r0, j0, tw, th;  // member, first interior ring column (0-based), first row, width, height
 };
+
+// mixed path, domains too large for the resident kernel: the multi-tile
+// kernel with the resident mixed kernel's precision; its per-step FP32
+// coefficients (MC_*), masks and FP32 velocity ping-pong live in scratch the
+// handle allocates (trop_multi_mixed_scratch_bytes)
+enum { MC_BXN, MC_BXS, MC_BYE, MC_BYW, MC_SAM, MC_COR, MC_UT, MC_VT, MC_PRHU, MC_RPRHT, MC_RDEN, MC_COUNT };
+struct MultiMixed {
+  float *cf;            // [MC_COUNT][n2]
+  unsigned char *fl;    // bit 0: lev_u >= 1, bit 1: lev_t >= 1
+  float *ub[2], *vb[2]; // barotropic velocities between substeps
+  float *vs0[2];        // the first substep's viscosity (u, v)
+};
+size_t trop_multi_mixed_scratch_bytes(long long n2);
+void trop_multi_mixed_bind(MultiMixed &M, void *scratch, long long n2);
+int trop_multi_mixed_max_blocks(int TX, int TY);
+cudaError_t launch_trop_multi_mixed(const Dev &P, const MultiMixed &M, const TileRef *dtiles, int ntiles, int TX,
+                                    int TY, int nblocks, unsigned long long *cnt, int *err, cudaStream_t s);
+
 size_t trop_batch_smem(int TX, int TY);
 int trop_batch_max_blocks(int TX, int TY);
 cudaError_t launch_trop_batch(const Dev *dPs, const TileRef *dtiles, int ntiles, int TX, int TY, int nblocks,

@@ -122,3 +122,39 @@ def test_global_sums(flags):
     assert ht == pytest.approx((tc * dv).sum(), rel=1e-12)
     assert sl == pytest.approx((sc * dv).sum(), rel=1e-12)
     m.close()
+
+
+def test_mixed_multi_tile_within_bounds():
+    """720 x 320 x 30 is too large for the resident kernel, so the mixed
+    handle runs the multi-tile mixed kernel (FP32 coefficients and
+    velocities between substeps); after 24 steps its error against the FP64
+    path is within the mixed bounds."""
+    c = make_case("global05")
+    md = Model(c)
+    mm = Model(c, flags=L.PCOM_PREC_MIXED)
+    md.run(24)
+    mm.run(24)
+    mm.check_finite()
+    err = errors(mm, md)
+    print("\nglobal05 mixed (multi-tile) after 24 steps:", {k: f"{v:.2e}" for k, v in err.items()})
+    for f, e in err.items():
+        assert e <= BOUNDS[f], f"{f} rel RMS {e:.3e} > {BOUNDS[f]:.0e}"
+    md.close()
+    mm.close()
+
+
+def test_mixed_multi_tile_matches_resident():
+    """On the 1-degree domain the mixed handle's two barotropic kernels (the
+    resident one and the multi-tile one, forced) do the same FP32/FP64
+    arithmetic: after 6 steps they agree far inside the mixed bounds."""
+    c = make_case("global1")
+    ms = [Model(c, flags=L.PCOM_PREC_MIXED) for _ in range(2)]
+    L.check(ms[1].lib.pcom_gpu_set_trop_kernel(ms[1].handle, 2), "set_trop_kernel")
+    for m in ms:
+        m.run(6)
+    err = errors(ms[1], ms[0])
+    print("\nglobal1 mixed multi-tile vs resident after 6 steps:", {k: f"{v:.2e}" for k, v in err.items()})
+    for f, e in err.items():
+        assert e <= 1e-2 * max(BOUNDS[f], 1e-7), f"{f} rel RMS {e:.3e}"
+    for m in ms:
+        m.close()
