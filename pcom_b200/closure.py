@@ -3,17 +3,29 @@ nested coarse grid, training of the tensor-core network (include/pcom_cnn.h)
 and coarse runs with and without it.
 
 Target.  For a sample time t the coarse model is started from the
-coarse-grained fine state CG(fine(t)) and stepped once (dt = the coarse
+coarse-grained fine state CG(fine(t)) and stepped k times (dt = the coarse
 baroclinic step); the target is the per-level tendency residual
-    (CG(fine(t + dt)) - coarse_step(CG(fine(t)))) / dt
+    (CG(fine(t + k dt)) - coarse_steps(CG(fine(t)))) / (k dt)
 for u, v, T and S, the part of the fine model's evolution the coarse model
 misses.  Inputs: u, v, T, S and the specific-volume anomaly per level, as
-5 channels of one image per level.  Closure run: after every coarse step the
-network's output (scaled back) is added as a tendency over the step.
+5 channels of one image per level.  Closure run: every `cadence` coarse
+steps the network's output (scaled back) is added as a tendency over
+cadence x dt.
 
-Usage (the experiment reported for the 1-degree grid):
-    python -m pcom_b200.closure --fine global025 --spinup-days 2 \
-        --train-days 8 --eval-days 2 --out closure_result.json
+Windows.  The fine run goes on through four consecutive windows: spin-up;
+training (samples every `every` coarse steps); validation (coarse runs with
+each output variant of VARIANTS, which picks the one applied); test (coarse
+runs of the chosen variant at each cadence, in the closure form's precision,
+beside the plain coarse model in FP64 and in that precision), judged by
+the RMS error against CG(fine) averaged over the window.  The SYPD of each
+form comes from CUDA-event timings of its step and of the network.
+
+Usage (configuration 5: a year of 0.25-degree training data, a year of
+coarse runs):
+    python -m pcom_b200.closure --fine global025 --spinup-days 10 \
+        --train-days 365 --every 24 --target-steps 3 --val-days 30 \
+        --test-days 365 --form-flags mixed --cadences 1,4,8 --epochs 15 \
+        --out closure_year.json
 """
 from __future__ import annotations
 
