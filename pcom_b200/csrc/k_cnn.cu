@@ -121,6 +121,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+// the same, without waiting: issue several, then tmem_ld_wait()
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // source pixel of tap t (0..8, dy = t/3 - 1, dx = t%3 - 1) for pixel p; -1 if padding
 __device__ __forceinline__ long long tap_src(long long p, int t, int H, int W, int periodic_x) {
   const long long hw = (long long)H * W;
@@ -267,16 +278,17 @@ constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 byt
 // Each role has its own warps and
 // they hand work to one another through mbarriers instead of CTA barriers
 // (six ring slots instead of four, so row loads run up to three tiles ahead):
-//   warps 0-3  epilogue: warp w drains lane quarter w of an accumulator
-//              (tcgen05.ld), frees it, applies bias + ReLU (or the ReLU mask)
-//              and stores the tile; 64-channel BF16 tiles go through a
+//   warps 0-7  epilogue: warp w drains half the columns (w / 4) of lane
+//              quarter w % 4 of an accumulator (tcgen05.ld, all issued
+//              before one wait), frees it, applies bias + ReLU (or the ReLU
+//              mask) and stores the tile; 64-channel BF16 tiles go through a
 //              double-buffered staging tile in the 128-byte swizzled layout
 //              and leave with one TMA tensor store (cp.async.bulk.tensor)
-//   warp 4     loads: streams each new halo row into its ring slot with
+//   warp 8     loads: streams each new halo row into its ring slot with
 //              cp.async, whose completion arrives on the slot's "full"
 //              mbarrier; reuses a slot once the MMAs reading its old row
 //              have completed ("empty" mbarrier, tcgen05.commit)
-//   warp 5     MMA: one thread waits for the tile's rows and a free
+//   warp 9     MMA: one thread waits for the tile's rows and a free
 //              accumulator, issues the 9 taps x CIN/16 MMAs and commits
 //              "accumulator full" and the release of the rows the next tile
 //              does not read.
@@ -285,7 +297,7 @@ constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 byt
 // bounded: a wait that gives up sets the error flag and a shared stop flag,
 // and every role leaves its loop; the MMA thread then waits (bounded) for its
 // MMAs before tensor memory is freed.
-constexpr int kWsThreads = 192;
+constexpr int kWsThreads = 320;  // 8 epilogue warps, 1 load warp, 1 MMA warp
 constexpr int kWsRing = 6;                     // halo row slots: loads run up to three tiles ahead
 constexpr int kPlaneW = kWsRing * kRowB + 16;  // padded ring plane (12,496 bytes)
 
@@ -318,7 +330,10 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
   constexpr int W_BYTES = 9 * NOUT * CIN * 2;
   constexpr int STG = kM * NOUT * 2;  // one staging tile
   constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
+  constexpr int NSPLIT = NOUT >= 32 ? 2 : 1;  // epilogue warps per lane quarter
+  constexpr int CPW = NOUT / NSPLIT;          // accumulator columns per epilogue warp
   extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ float s_bias[NOUT];
   __shared__ __align__(8) uint64_t full[kWsRing], empty[kWsRing], accf[2], acce[2], sfree[2], swritten[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int s_stop;
@@ -344,9 +359,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
     }
     for (int q = 0; q < 2; ++q) {
       mbar_init(smem_u32(&accf[q]), 1);
-      mbar_init(smem_u32(&acce[q]), 4);        // one per epilogue warp
-      mbar_init(smem_u32(&sfree[q]), 1);       // staging tile q read by its last store
-      mbar_init(smem_u32(&swritten[q]), 128);  // staging tile q written by the epilogue
+      mbar_init(smem_u32(&acce[q]), 4 * NSPLIT);      // one per epilogue warp
+      mbar_init(smem_u32(&sfree[q]), 1);              // staging tile q read by its last store
+      mbar_init(smem_u32(&swritten[q]), 128 * NSPLIT);  // staging tile q written by the epilogue
     }
     mbar_init(smem_u32(&done), 1);
     s_stop = 0;
@@ -358,6 +373,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
     cp_async16(Wsm + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16),
                w + ((long long)t * NOUT + n) * CIN + c * 8, true);
   }
+  for (int q = tid; q < NOUT; q += kWsThreads) s_bias[q] = mode == 2 ? 0.f : bias[q];
   cp_async_wait_all();
   fence_async_smem();
   tc_fence_before();
@@ -390,7 +406,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
     atomicExch(err, 1);
   };
 
-  if (warp == 4) {
+  if (warp == 8) {
     // ---------------------------------------------------------------- loads
     int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
     for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
@@ -428,7 +444,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
       }
     }
     cp_async_wait_all();
-  } else if (warp == 5) {
+  } else if (warp == 9) {
     // ------------------------------------------------------------------ MMA
     if (lane == 0) {
       constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
@@ -494,66 +510,71 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
     }
   } else {
     // ------------------------------------------------------------- epilogue
-    const int quarter = warp;  // lane quarter of the accumulator
+    const int quarter = warp & 3, half = warp >> 2;  // lane quarter, column half
     const int m = quarter * 32 + lane;
+    const int c_lo = half * CPW;                       // this warp's first column
     Pos a = first;
     int it = 0;
-    for (long long tile = t0; tile < t1 && !s_stop; ++tile, ++it, a = advance(a)) {
+    for (long long tile = t0; tile < t1 && !s_stop && half < NSPLIT; ++tile, ++it, a = advance(a)) {
       const int b = it & 1;
       const int x0 = a.tx * kM, x = x0 + m;
       const long long p = (long long)a.gr * W + x;
-      // the ReLU mask of this pixel, fetched before the wait
-      uint4 am[NOUT / 8];
+      // the ReLU mask of this pixel's columns, fetched before the wait
+      uint4 am[CPW / 8];
       if (mode == 2) {
         #pragma unroll
-        for (int c = 0; c < NOUT / 8; ++c)
-          am[c] = x < W ? __ldg(reinterpret_cast<const uint4 *>(aux + p * NOUT) + c) : make_uint4(0, 0, 0, 0);
+        for (int c = 0; c < CPW / 8; ++c)
+          am[c] = x < W ? __ldg(reinterpret_cast<const uint4 *>(aux + p * NOUT + c_lo) + c) : make_uint4(0, 0, 0, 0);
       }
       const bool ok = mbar_wait(smem_u32(&accf[b]), (uint32_t)((it >> 1) & 1));
       if (!ok) stop();
       if (__any_sync(0xffffffffu, !ok)) break;
       tc_fence_after();
-      float v[NOUT];
-      const uint32_t lane_addr = tmem + (uint32_t)b * NCOLS + ((uint32_t)(quarter * 32) << 16);
+      uint32_t r[CPW];
+      const uint32_t lane_addr = tmem + (uint32_t)b * NCOLS + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c_lo;
       #pragma unroll
-      for (int c0 = 0; c0 < NOUT; c0 += 16) tmem_ld16(lane_addr + c0, v + c0);
+      for (int c0 = 0; c0 < CPW; c0 += 16) tmem_ld16_nowait(lane_addr + c0, r + c0);
+      tmem_ld_wait();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
       if (mode == 1) {
-        if (x < W) {
+        if (x < W && c_lo < nstore) {
           float *o = (float *)out + p * nstore;
-          if (nstore == 4) {
-            *reinterpret_cast<float4 *>(o) = make_float4(v[0] + bias[0], v[1] + bias[1], v[2] + bias[2], v[3] + bias[3]);
+          if (nstore == 4 && c_lo == 0) {
+            *reinterpret_cast<float4 *>(o) =
+                make_float4(__uint_as_float(r[0]) + s_bias[0], __uint_as_float(r[1]) + s_bias[1],
+                            __uint_as_float(r[2]) + s_bias[2], __uint_as_float(r[3]) + s_bias[3]);
           } else {
             #pragma unroll
-            for (int q = 0; q < NOUT; ++q)
-              if (q < nstore) o[q] = v[q] + bias[q];
+            for (int q = 0; q < CPW; ++q)
+              if (c_lo + q < nstore) o[c_lo + q] = __uint_as_float(r[q]) + s_bias[c_lo + q];
           }
         }
         continue;
       }
-      uint32_t pk[NOUT / 2];
+      uint32_t pk[CPW / 2];
       #pragma unroll
-      for (int q = 0; q < NOUT / 2; ++q) {
+      for (int q = 0; q < CPW / 2; ++q) {
+        const float v0 = __uint_as_float(r[2 * q]), v1 = __uint_as_float(r[2 * q + 1]);
         float lo, hi;
         if (mode == 0) {
-          lo = fmaxf(v[2 * q] + bias[2 * q], 0.f);
-          hi = fmaxf(v[2 * q + 1] + bias[2 * q + 1], 0.f);
+          lo = fmaxf(v0 + s_bias[c_lo + 2 * q], 0.f);
+          hi = fmaxf(v1 + s_bias[c_lo + 2 * q + 1], 0.f);
         } else {
           const uint32_t aw = (&am[q / 4].x)[q % 4];
           const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
-          lo = __low2float(a2) > 0.f ? v[2 * q] : 0.f;
-          hi = __high2float(a2) > 0.f ? v[2 * q + 1] : 0.f;
+          lo = __low2float(a2) > 0.f ? v0 : 0.f;
+          hi = __high2float(a2) > 0.f ? v1 : 0.f;
         }
         const __nv_bfloat162 b2 = __floats2bfloat162_rn(lo, hi);
         pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
       }
       if (!tma) {
         if (x < W) {
-          uint4 *o = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + p * NOUT);
+          uint4 *o = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + p * NOUT + c_lo);
           #pragma unroll
-          for (int c = 0; c < NOUT / 8; ++c) o[c] = make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+          for (int c = 0; c < CPW / 8; ++c) o[c] = make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
         }
         continue;
       }
@@ -572,9 +593,11 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
       }
       uint8_t *row = stg_p + sb * STG + m * 128;
       #pragma unroll
-      for (int c = 0; c < 8; ++c)  // 16-byte chunk c of the pixel's 128 bytes, 128-byte swizzle
-        *reinterpret_cast<uint4 *>(row + ((c ^ (m & 7)) << 4)) =
+      for (int c = 0; c < CPW / 8; ++c) {  // 16-byte chunk cc of the pixel's 128 bytes, 128-byte swizzle
+        const int cc = c_lo / 8 + c;
+        *reinterpret_cast<uint4 *>(row + ((cc ^ (m & 7)) << 4)) =
             make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+      }
       fence_async_smem();
       mbar_arrive(smem_u32(&swritten[sb]));
       if (tid == 0) {
