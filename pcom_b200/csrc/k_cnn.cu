@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
       mbar_init(smem_u32(&accf[q]), 1);
       mbar_init(smem_u32(&acce[q]), 4 * NSPLIT);      // one per epilogue warp
       mbar_init(smem_u32(&sfree[q]), 1);              // staging tile q read by its last store
-      mbar_init(smem_u32(&swritten[q]), 128 * NSPLIT);  // staging tile q written by the epilogue
+      mbar_init(smem_u32(&swritten[q]), 4 * NSPLIT);  // staging tile q written (one arrival per epilogue warp)
     }
     mbar_init(smem_u32(&done), 1);
     s_stop = 0;
@@ -598,8 +598,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
         *reinterpret_cast<uint4 *>(row + ((cc ^ (m & 7)) << 4)) =
             make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
       }
-      fence_async_smem();
-      mbar_arrive(smem_u32(&swritten[sb]));
+      fence_async_smem();  // this thread's staging writes, ordered before the TMA store reads them
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&swritten[sb]));
       if (tid == 0) {
         if (!mbar_wait(smem_u32(&swritten[sb]), (uint32_t)((it >> 1) & 1))) {
           stop();
