@@ -34,7 +34,7 @@
 
 namespace {
 
-constexpr long long kSpin = 1LL << 22;  // try_wait suspends in hardware between polls
+constexpr long long kSpin = 1LL << 26;  // polls of an mbarrier before a wait gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -74,12 +74,16 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
 }
 
-// bounded wait for phase `parity` of an mbarrier
+// bounded wait for phase `parity` of an mbarrier.  test_wait polls without
+// suspending the thread (try_wait may suspend it for a system-dependent
+// time, which put microseconds on every hand-off between the warps of the
+// persistent convolution); the iteration cap bounds the wait to well under
+// a second.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   for (long long it = 0; it < kSpin; ++it) {
     uint32_t done;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, p;\n\t}\n"
         : "=r"(done)
         : "r"(mbar), "r"(parity)
