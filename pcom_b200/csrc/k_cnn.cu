@@ -477,6 +477,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
           stop();
           break;
         }
+        // the rows arrived through cp.async (generic proxy); the MMAs read
+        // them through the async proxy
+        fence_async_smem();
         tc_fence_after();
         uint32_t accum = 0;
         #pragma unroll
