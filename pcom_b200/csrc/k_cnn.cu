@@ -288,11 +288,14 @@ constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 byt
 //              mask) and stores the tile; 64-channel BF16 tiles go through a
 //              double-buffered staging tile in the 128-byte swizzled layout
 //              and leave with one TMA tensor store (cp.async.bulk.tensor)
-//   warp 8     loads: streams each new halo row into its ring slot with
+//   warps 8-11 loads: stream each new halo row into its ring slot with
 //              cp.async, whose completion arrives on the slot's "full"
-//              mbarrier; reuses a slot once the MMAs reading its old row
-//              have completed ("empty" mbarrier, tcgen05.commit)
-//   warp 9     MMA: one thread waits for the tile's rows and a free
+//              mbarrier; reuse a slot once the MMAs reading its old row have
+//              completed ("empty" mbarrier, tcgen05.commit).  One warp's
+//              cp.async stream delivered a 16.6 KB row per ~5,500 cycles,
+//              slower than the tile's MMAs (clock64 timestamps per role);
+//              four keep the MMA thread supplied
+//   warp 12    MMA: one thread waits for the tile's rows and a free
 //              accumulator, issues the 9 taps x CIN/16 MMAs and commits
 //              "accumulator full" and the release of the rows the next tile
 //              does not read.
@@ -301,7 +304,8 @@ constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 byt
 // bounded: a wait that gives up sets the error flag and a shared stop flag,
 // and every role leaves its loop; the MMA thread then waits (bounded) for its
 // MMAs before tensor memory is freed.
-constexpr int kWsThreads = 320;  // 8 epilogue warps, 1 load warp, 1 MMA warp
+constexpr int kLoadWarps = 4;    // one warp's cp.async stream cannot keep a row per tile in flight
+constexpr int kWsThreads = (8 + kLoadWarps + 1) * 32;  // 8 epilogue warps, the load warps, 1 MMA warp
 constexpr int kWsRing = 6;                     // halo row slots: loads run up to three tiles ahead
 constexpr int kPlaneW = kWsRing * kRowB + 16;  // padded ring plane (12,496 bytes)
 
@@ -358,7 +362,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
   if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), 2 * NCOLS);
   if (tid == 0) {
     for (int q = 0; q < kWsRing; ++q) {
-      mbar_init(smem_u32(&full[q]), 32);  // one arrival per load-warp lane
+      mbar_init(smem_u32(&full[q]), 32 * kLoadWarps);  // one arrival per load thread
       mbar_init(smem_u32(&empty[q]), 1);
     }
     for (int q = 0; q < 2; ++q) {
@@ -410,8 +414,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
     atomicExch(err, 1);
   };
 
-  if (warp == 8) {
+  if (warp >= 8 && warp < 8 + kLoadWarps) {
     // ---------------------------------------------------------------- loads
+    const int lt = tid - 8 * 32;  // load thread 0 .. 32 * kLoadWarps - 1
     int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
     for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
     Pos a = first;
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
           break;
         }
         const int x0 = a.tx * kM;
-        for (int q = lane; q < kHaloW * KC; q += 32) {
+        for (int q = lt; q < kHaloW * KC; q += 32 * kLoadWarps) {
           const int u = q / KC, c = q % KC;
           int xx = x0 - 1 + u;
           bool ok = true;
@@ -448,7 +453,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
       }
     }
     cp_async_wait_all();
-  } else if (warp == 9) {
+  } else if (warp == 8 + kLoadWarps) {
     // ------------------------------------------------------------------ MMA
     if (lane == 0) {
       constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
