@@ -429,6 +429,32 @@ def run_mixed_leg(args, case, stream, steps):
             "rel_rms_error_vs_fp64_after_24_steps": {k_: float(f"{v:.3e}") for k_, v in err.items()}}
 
 
+def device_ms_per_step(m, stream, steps: int, warmup: int) -> float:
+    """CUDA-event time per step of `steps` device-resident steps (den_prho on
+    day change) after `warmup` steps through the host driver."""
+    import torch
+
+    from pcom_b200 import _lib as L
+
+    m.set_stream(stream.cuda_stream)
+    m.run(max(warmup, 3))
+    it0 = m.iter
+    day_of = lambda it: (it - 1) * STEP_SECONDS // 86400
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for q in range(steps):
+        it = it0 + 1 + q
+        if day_of(it) != day_of(it - 1):
+            L.check(m.lib.pcom_gpu_den_prho(m.handle), "den_prho")
+        L.check(m.lib.pcom_gpu_step_async(m.handle, it), "step")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    m.check_finite()
+    return e0.elapsed_time(e1) / steps
+
+
 CLOSURE_CADENCE = 8  # the closure form: the network every 8 coarse steps (tendency over 8 dt)
 
 
