@@ -34,7 +34,9 @@
 
 namespace {
 
-constexpr long long kSpin = 1LL << 26;  // polls of an mbarrier before a wait gives up
+// polls of an mbarrier before a wait gives up: try_wait may suspend between
+// polls (a system-dependent time), test_wait returns at once
+constexpr long long kSpin = 1LL << 22, kSpinPoll = 1LL << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -74,13 +76,26 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
 }
 
-// bounded wait for phase `parity` of an mbarrier.  test_wait polls without
-// suspending the thread (try_wait may suspend it for a system-dependent
-// time, which put microseconds on every hand-off between the warps of the
-// persistent convolution); the iteration cap bounds the wait to well under
-// a second.
+// bounded wait for phase `parity` of an mbarrier.  try_wait may suspend the
+// thread until the phase completes, so waiting warps give their issue slots
+// to the warps that work; mbar_spin polls with test_wait instead, for the
+// one thread whose wake-up latency is on the critical path (the MMA issuer
+// of the persistent convolution).
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   for (long long it = 0; it < kSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ bool mbar_spin(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kSpinPoll; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -295,7 +310,9 @@ constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 byt
 //              cp.async stream delivered a 16.6 KB row per ~5,500 cycles,
 //              slower than the tile's MMAs (clock64 timestamps per role);
 //              four keep the MMA thread supplied
-//   warp 12    MMA: one thread waits for the tile's rows and a free
+//   warp 12    MMA: one thread (the only one that polls: the others wait
+//              suspended, which leaves it the issue slots; with every waiter
+//              polling, it took ~95 cycles to issue each MMA) waits for the tile's rows and a free
 //              accumulator, issues the 9 taps x CIN/16 MMAs and commits
 //              "accumulator full" and the release of the rows the next tile
 //              does not read.
@@ -474,10 +491,10 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
           tag_row[s] = r;
           tag_tx[s] = a.tx;
           ++nload[s];
-          ok = mbar_wait(smem_u32(&full[s]), (uint32_t)((nload[s] - 1) & 1));
+          ok = mbar_spin(smem_u32(&full[s]), (uint32_t)((nload[s] - 1) & 1));
         }
         // accumulator b was last drained for tile it - 2
-        if (ok && it >= 2) ok = mbar_wait(smem_u32(&acce[b]), (uint32_t)(((it >> 1) - 1) & 1));
+        if (ok && it >= 2) ok = mbar_spin(smem_u32(&acce[b]), (uint32_t)(((it >> 1) - 1) & 1));
         if (!ok) {
           stop();
           break;
