@@ -52,6 +52,23 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
+// The same for the 128-byte swizzled K-major layout (rows of 128 bytes, the
+// 16-byte chunks of row r at position c ^ (r % 8), 1024-byte atoms of 8
+// rows): stride byte offset = 1024 (8-row groups), leading byte offset
+// unused (1), layout type 2 at bit 61, and the base offset (bits 49-51) =
+// the start address's row phase within its atom, for operands that start
+// a whole number of rows into an atom.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)((saddr >> 7) & 7u) << 49;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
 // Instruction descriptor for kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
 // (bits 7-9 = 1, 10-12 = 1), A/B major (bit 15/16: 0 = K, 1 = MN),
 // N >> 3 at bits 17-22, M >> 4 at bits 24-28.
@@ -325,6 +342,16 @@ constexpr int kLoadWarps = 4;    // one warp's cp.async stream cannot keep a row
 constexpr int kWsThreads = (8 + kLoadWarps + 1) * 32;  // 8 epilogue warps, the load warps, 1 MMA warp
 constexpr int kWsRing = 6;                     // halo row slots: loads run up to three tiles ahead
 constexpr int kPlaneW = kWsRing * kRowB + 16;  // padded ring plane (12,496 bytes)
+// 64-channel inputs: a slot is 130 pixel rows of 128 bytes in the 128-byte
+// swizzled layout, 1024-byte aligned (17 KB), so a tap's one-pixel shift
+// moves the A operand by whole 128-byte rows; in the plane layout the
+// shifted operand started 16 or 32 bytes into its 128-byte core matrices
+// and each MMA read took about twice as long
+constexpr int kSlotSW = 17 * 1024;
+template <int CIN>
+__host__ __device__ constexpr bool ring_sw() { return CIN == 64; }
+template <int CIN>
+__host__ __device__ constexpr int ring_bytes() { return ring_sw<CIN>() ? kWsRing * kSlotSW : (CIN / 8) * kPlaneW; }
 
 __device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
@@ -367,6 +394,7 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   uint8_t *const sbase = smem_raw + (base - smem_u32(smem_raw));
   const bool tma = ws_tma<CIN, NOUT>() && mode != 1;
+  static_assert(!ring_sw<CIN>() || (W_BYTES % 1024 == 0 && STG % 1024 == 0), "swizzled ring slots need 1024-byte alignment");
   const uint32_t Stg = base, Wsm = base + (ws_tma<CIN, NOUT>() ? 2 * STG : 0), Ring = Wsm + W_BYTES;
   uint8_t *const stg_p = sbase;
   const int ntx = (W + kM - 1) / kM;
@@ -460,8 +488,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
               ok = false;
             }
           }
-          cp_async16(Ring + (uint32_t)(c * kPlaneW + s * kRowB + u * 16),
-                     ok ? (const void *)(in + ((long long)r * W + xx) * CIN + c * 8) : (const void *)in, ok);
+          const uint32_t dst = ring_sw<CIN>() ? Ring + (uint32_t)(s * kSlotSW + u * 128 + ((c ^ (u & 7)) << 4))
+                                              : Ring + (uint32_t)(c * kPlaneW + s * kRowB + u * 16);
+          cp_async16(dst, ok ? (const void *)(in + ((long long)r * W + xx) * CIN + c * 8) : (const void *)in, ok);
         }
         cp_async_arrive_noinc(smem_u32(&full[s]));
         tag_row[s] = r;
@@ -511,7 +540,9 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
           const int s = (a.gr + dy) % kWsRing;
           #pragma unroll
           for (int j = 0; j < CIN / 16; ++j) {
-            const uint64_t ad = adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kPlaneW) >> 4);
+            const uint64_t ad = ring_sw<CIN>()
+                                    ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW + (dx + 1) * 128 + j * 32))
+                                    : adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kPlaneW) >> 4);
             const uint64_t bd = bdesc0 + (uint64_t)((tp * NOUT * CIN * 2 + j * 256) >> 4);
             umma_bf16(tmem + (uint32_t)b * NCOLS, ad, bd, idesc, accum);
             accum = 1u;
@@ -764,7 +795,7 @@ size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 
 template <int CIN, int NOUT>
 size_t ws_smem() {
   return 1024 + (ws_tma<CIN, NOUT>() ? 2 * (size_t)kM * NOUT * 2 : 0) + (size_t)9 * NOUT * CIN * 2 +
-         (size_t)(CIN / 8) * kPlaneW;  // 64 -> 64: 1 + 32 + 72 + 97.6 KB
+         (size_t)ring_bytes<CIN>();  // 64 -> 64: 1 + 32 + 72 + 102 KB
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry-point table (the
