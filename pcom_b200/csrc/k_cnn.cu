@@ -55,16 +55,17 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 // The same for the 128-byte swizzled K-major layout (rows of 128 bytes, the
 // 16-byte chunks of row r at position c ^ (r % 8), 1024-byte atoms of 8
 // rows): stride byte offset = 1024 (8-row groups), leading byte offset
-// unused (1), layout type 2 at bit 61, and the base offset (bits 49-51) =
-// the start address's row phase within its atom, for operands that start
-// a whole number of rows into an atom.
+// unused (1), layout type 2 at bit 61, base offset 0.  The swizzle follows
+// the absolute shared-memory address, so an operand may start a whole
+// number of rows into an atom with base offset 0 (checked against a CPU
+// convolution on the B200; the start address's row phase in the base
+// offset field gave wrong results).
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
   d |= (uint64_t)1 << 16;
   d |= (uint64_t)(1024 >> 4) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)((saddr >> 7) & 7u) << 49;
   d |= (uint64_t)2 << 61;
   return d;
 }
