@@ -4,14 +4,17 @@
 // residuals), trained and evaluated with the kernels below.
 //
 // Every convolution is an implicit GEMM on the 5th-generation tensor cores:
-// BF16 operands staged in shared memory in the UMMA "interleave" (no
-// swizzle) canonical layout, one elected thread issuing tcgen05.mma
+// BF16 operands staged in shared memory in a UMMA canonical layout (128-byte
+// swizzle for 64-channel rows brought in by TMA tensor loads, "interleave"
+// without swizzle otherwise), one elected thread issuing tcgen05.mma
 // (kind::f16, FP32 accumulation in tensor memory), completion tracked with
-// tcgen05.commit on an mbarrier, and the epilogue reading the accumulator
-// with tcgen05.ld.  Forward and data-gradient convolutions are K-major GEMMs
-// (rows = pixels, K = tap x input channel, N = output channels); the weight
-// gradient is an MN-major GEMM (rows = tap x input channel, N = output
-// channels, K = pixels) split over CTAs with FP32 atomics.
+// tcgen05.commit on mbarriers, and the epilogue reading the accumulator
+// with tcgen05.ld and writing 64-channel rows with TMA tensor stores.
+// Forward and data-gradient convolutions are K-major GEMMs (rows = pixels,
+// K = input channel, N = the three row taps x output channels, summed over
+// the three column taps); the weight gradient is an MN-major GEMM (rows =
+// tap x input channel, N = output channels, K = pixels) split over CTAs with
+// FP32 atomics.
 //
 // Activations are NHWC over images of H x W pixels (one image per model
 // level), channels contiguous: 16 (the 5 inputs, zero-padded) or 64.
@@ -296,63 +299,68 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(const __nv_bfloat16 *__res
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
 
-// Ring geometry of the persistent convolution below: a tile is 128
-// consecutive pixels of one image row, its halo rows hold 130 pixels, stored
-// "chunk-planar" (plane c holds channels 8c..8c+7, 16 bytes per pixel).
-constexpr int kHaloW = kM + 2;               // halo columns
-constexpr int kRowB = kHaloW * 16;           // one slot of one plane (2,080 bytes)
-
 // ----------------------------------------------------------------------------
-// Persistent convolution (the form every whole-image convolution takes).
-// Each CTA walks a contiguous strip of tiles down the rows of one column of
-// tiles, so consecutive tiles share two of their three halo rows: the rows
-// live in a ring of slots, each tile loads one new row, and the A operand of
-// tap (dy, dx) is the planes of the slot holding row y + dy read from pixel
-// dx + 1 (leading byte offset = plane stride, stride byte offset = 128 bytes
-// = 8 pixels).  Taps whose row falls outside the image are skipped.  All 9
-// taps of the weights stay in shared memory.  Two accumulators in tensor
-// memory let the MMAs of one tile run while the previous one is drained.
-// Each role has its own warps and
-// they hand work to one another through mbarriers instead of CTA barriers
-// (six ring slots instead of four, so row loads run up to three tiles ahead):
-//   warps 0-7  epilogue: warp w drains half the columns (w / 4) of lane
-//              quarter w % 4 of an accumulator (tcgen05.ld, all issued
-//              before one wait), frees it, applies bias + ReLU (or the ReLU
-//              mask) and stores the tile; 64-channel BF16 tiles go through a
-//              double-buffered staging tile in the 128-byte swizzled layout
-//              and leave with one TMA tensor store (cp.async.bulk.tensor)
-//   warps 8-11 loads: stream each new halo row into its ring slot with
-//              cp.async, whose completion arrives on the slot's "full"
-//              mbarrier; reuse a slot once the MMAs reading its old row have
-//              completed ("empty" mbarrier, tcgen05.commit).  One warp's
-//              cp.async stream delivered a 16.6 KB row per ~5,500 cycles,
-//              slower than the tile's MMAs (clock64 timestamps per role);
-//              four keep the MMA thread supplied
-//   warp 12    MMA: one thread (the only one that polls: the others wait
-//              suspended, which leaves it the issue slots; with every waiter
-//              polling, it took ~95 cycles to issue each MMA) waits for the tile's rows and a free
-//              accumulator, issues the 9 taps x CIN/16 MMAs and commits
-//              "accumulator full" and the release of the rows the next tile
-//              does not read.
-// The plane stride of the ring is padded by 16 bytes so a load warp's eight
-// 16-byte chunks of one pixel land in different banks.  Every wait is
-// bounded: a wait that gives up sets the error flag and a shared stop flag,
-// and every role leaves its loop; the MMA thread then waits (bounded) for its
-// MMAs before tensor memory is freed.
-constexpr int kLoadWarps = 4;    // one warp's cp.async stream cannot keep a row per tile in flight
-constexpr int kWsThreads = (8 + kLoadWarps + 1) * 32;  // 8 epilogue warps, the load warps, 1 MMA warp
-constexpr int kWsRing = 6;                     // halo row slots: loads run up to three tiles ahead
-constexpr int kPlaneW = kWsRing * kRowB + 16;  // padded ring plane (12,496 bytes)
-// 64-channel inputs: a slot is 130 pixel rows of 128 bytes in the 128-byte
-// swizzled layout, 1024-byte aligned (17 KB), so a tap's one-pixel shift
-// moves the A operand by whole 128-byte rows; in the plane layout the
-// shifted operand started 16 or 32 bytes into its 128-byte core matrices
-// and each MMA read took about twice as long
-constexpr int kSlotSW = 17 * 1024;
+// Persistent row-streaming convolution (the form every whole-image
+// convolution takes).
+//
+// A tile is 128 consecutive pixels of one image row (tile column tx covers
+// pixels 128 tx ..); each CTA owns a contiguous run of output rows of one or
+// two tile columns.  Instead of gathering three input rows per output row,
+// it streams every input row once and multiplies it by the weights of all
+// three row taps at once: for input row i the B operand stacks the weights
+// of taps dy = -1, 0, +1 (target t = dy + 1), so one MMA with N = 3 x BW
+// (BW = the output channels, at least 32) adds the contributions of row i to
+// output rows i + 1, i and i - 1.  Output rows live in a ring of 8
+// accumulator blocks of BW columns in tensor memory, output q of the CTA in
+// block 7 - (q % 8): the blocks of outputs i + 1, i, i - 1 are then adjacent
+// (lowest column first), except where the ring wraps, where the MMA is split
+// in two.  The first contribution to an output row is the MMA that starts
+// its block (accumulate = 0), issued as its own MMA where its neighbours
+// accumulate.  The one thread that issues MMAs is the limit of this kernel:
+// a tcgen05.mma of M = 128 took ~110 cycles to issue whatever its N up to
+// 192 (operands at a new address each time), so N = 192 does three times
+// the work of N = 64 in the same issue slot.  Per 64-channel input row:
+// 3 column taps x 4 K steps = 12 MMAs (plus the splits).
+//
+// Roles (warps), handing work over through mbarriers:
+//   warps 0-7   epilogue: output q goes to the four warps of parity q % 2,
+//               warp w draining lane quarter w % 4 (32 pixels, all
+//               columns) with tcgen05.ld, freeing the block, applying bias +
+//               ReLU (or the ReLU mask) and storing; 64-channel BF16 rows go
+//               through the warp's own 4 KB staging tile in the 128-byte
+//               swizzled layout and one TMA tensor store per warp
+//   warps 8-11  loads.  64-channel inputs: warp 8 brings each 130-pixel
+//               input row (tile + one halo pixel each side) into its ring
+//               slot with one TMA tensor load (128-byte swizzle, zero fill
+//               outside the image); warp 9 waits for it, writes the
+//               wrapped-around halo pixel of a zonally periodic grid (which
+//               the tensor load fills with zero) and releases the slot to
+//               the MMA thread.  16-channel inputs: the four warps stream the
+//               row with cp.async into 8-channel planes (no swizzle).
+//   warp 12     MMA: one thread waits for the row and for the blocks it
+//               starts to be drained, issues the MMAs, and commits the
+//               release of the slot and "block full" for each output row
+//               the row completes.
+// Every wait is bounded: a wait that gives up sets the error flag and a
+// shared stop flag, and every role leaves its loop; the MMA thread waits
+// (bounded) for its MMAs and the load warp for its tensor loads before
+// tensor memory is freed and the CTA exits.
+constexpr int kRing = 6;           // input row slots
+constexpr int kBlocks = 8;         // accumulator blocks (output rows) in tensor memory
+constexpr int kRowPix = kM + 2;    // pixels per input row slot
+constexpr int kRowB = kRowPix * 16;            // plane layout: one slot of one plane (2,080 bytes)
+constexpr int kPlaneW = kRing * kRowB + 16;    // padded plane (12,496 bytes)
+constexpr int kSlotSW = 17 * 1024;             // swizzled layout: 130 rows of 128 bytes, 1024-byte aligned
+constexpr int kRowsThreads = 13 * 32;          // 8 epilogue + 4 load + 1 MMA warps
+
 template <int CIN>
-__host__ __device__ constexpr bool ring_sw() { return CIN == 64; }
+__host__ __device__ constexpr bool row_tma() { return CIN == 64; }
 template <int CIN>
-__host__ __device__ constexpr int ring_bytes() { return ring_sw<CIN>() ? kWsRing * kSlotSW : (CIN / 8) * kPlaneW; }
+__host__ __device__ constexpr int ring_bytes() { return row_tma<CIN>() ? kRing * kSlotSW : (CIN / 8) * kPlaneW; }
+template <int NOUT>
+__host__ __device__ constexpr int blk_w() { return NOUT < 32 ? 32 : NOUT; }
+template <int NOUT>
+__host__ __device__ constexpr bool store_tma() { return NOUT == 64; }
 
 __device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
@@ -360,124 +368,188 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar) {
 __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(mbar)
+      : "memory");
+}
 __device__ __forceinline__ void tma_store3(const CUtensorMap *map, uint32_t src, int c0, int c1, int c2) {
   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(map),
                "r"(src), "r"(c0), "r"(c1), "r"(c2)
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-template <int CIN, int NOUT>
-__host__ __device__ constexpr bool ws_tma() { return NOUT == 64; }
+// One tile column's run of output rows [rb, re] (global image rows, all
+// images stacked) out of a CTA's tiles [t, t1); tiles are numbered tile
+// column first.  Its input rows are rb - 1 .. re + 1, those of the same
+// images.
+struct RowRun {
+  int tx, rb, re, ilo, ihi;
+};
+__device__ __forceinline__ bool next_run(long long &t, long long t1, int NR, int H, RowRun &r) {
+  if (t >= t1) return false;
+  r.tx = (int)(t / NR);
+  r.rb = (int)(t % NR);
+  long long end = (long long)(r.tx + 1) * NR;
+  if (end > t1) end = t1;
+  r.re = r.rb + (int)(end - t) - 1;
+  r.ilo = r.rb - (r.rb % H > 0 ? 1 : 0);
+  r.ihi = r.re + (r.re % H < H - 1 ? 1 : 0);
+  t = end;
+  return true;
+}
 
 template <int CIN, int NOUT>
-__global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__restrict__ in,
-                                                        const __nv_bfloat16 *__restrict__ w,
-                                                        const float *__restrict__ bias,
-                                                        const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
-                                                        int H, int W, int periodic_x, int mode, int nstore, int *err,
-                                                        const __grid_constant__ CUtensorMap tmap) {
+__global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 *__restrict__ in,
+                                                            const __nv_bfloat16 *__restrict__ w,
+                                                            const float *__restrict__ bias,
+                                                            const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
+                                                            int H, int W, int periodic_x, int mode, int nstore,
+                                                            int *err, const __grid_constant__ CUtensorMap tmap_in,
+                                                            const __grid_constant__ CUtensorMap tmap_out) {
   constexpr int KC = CIN / 8;
-  constexpr int W_BYTES = 9 * NOUT * CIN * 2;
-  constexpr int STG = kM * NOUT * 2;  // one staging tile
-  constexpr uint32_t NCOLS = NOUT < 32 ? 32 : NOUT;
-  constexpr int NSPLIT = NOUT >= 32 ? 2 : 1;  // epilogue warps per lane quarter
-  constexpr int CPW = NOUT / NSPLIT;          // accumulator columns per epilogue warp
+  constexpr int BW = blk_w<NOUT>();
+  constexpr int WT_BYTES = BW * CIN * 2;      // one target's weights of one column tap
+  constexpr int W_BYTES = 9 * WT_BYTES;       // [column tap][target][BW rows][CIN]
+  constexpr int STG = 32 * NOUT * 2;          // one epilogue warp's staging tile
+  constexpr uint32_t NCOLS = kBlocks * BW;
+  constexpr uint32_t ROW_TX = kRowPix * 128;  // bytes of one 64-channel tensor load
+  static_assert(!row_tma<CIN>() || (W_BYTES % 1024 == 0 && STG % 1024 == 0), "swizzled slots need 1024-byte alignment");
+  static_assert(3 * BW <= 256, "N of one MMA");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ float s_bias[NOUT];
-  __shared__ __align__(8) uint64_t full[kWsRing], empty[kWsRing], accf[2], acce[2], sfree[2], swritten[2], done;
+  __shared__ __align__(8) uint64_t full[kRing], tmab[kRing], empty[kRing], bfull[kBlocks], bempty[kBlocks], done;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int s_stop;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  // 1024-byte aligned base: the swizzled staging tiles need it
+  // 1024-byte aligned base: swizzled staging tiles and ring slots need it
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   uint8_t *const sbase = smem_raw + (base - smem_u32(smem_raw));
-  const bool tma = ws_tma<CIN, NOUT>() && mode != 1;
-  static_assert(!ring_sw<CIN>() || (W_BYTES % 1024 == 0 && STG % 1024 == 0), "swizzled ring slots need 1024-byte alignment");
-  const uint32_t Stg = base, Wsm = base + (ws_tma<CIN, NOUT>() ? 2 * STG : 0), Ring = Wsm + W_BYTES;
-  uint8_t *const stg_p = sbase;
+  const bool tma_out = store_tma<NOUT>() && mode != 1;
+  const uint32_t Stg = base, Wsm = base + (store_tma<NOUT>() ? 8 * STG : 0), Ring = Wsm + W_BYTES;
   const int ntx = (W + kM - 1) / kM;
-  const long long NR = (long long)nimg * H;
-  const long long ntiles = NR * ntx;
+  const int NR = nimg * H;
+  const long long ntiles = (long long)NR * ntx;
   const long long chunk = (ntiles + gridDim.x - 1) / gridDim.x;
   const long long t0 = (long long)blockIdx.x * chunk;
   const long long t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
 
-  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), 2 * NCOLS);
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), NCOLS);
   if (tid == 0) {
-    for (int q = 0; q < kWsRing; ++q) {
-      mbar_init(smem_u32(&full[q]), 32 * kLoadWarps);  // one arrival per load thread
+    for (int q = 0; q < kRing; ++q) {
+      mbar_init(smem_u32(&full[q]), row_tma<CIN>() ? 1 : 32 * 4);  // halo writer, or one arrival per load thread
+      mbar_init(smem_u32(&tmab[q]), 1);
       mbar_init(smem_u32(&empty[q]), 1);
     }
-    for (int q = 0; q < 2; ++q) {
-      mbar_init(smem_u32(&accf[q]), 1);
-      mbar_init(smem_u32(&acce[q]), 4 * NSPLIT);      // one per epilogue warp
-      mbar_init(smem_u32(&sfree[q]), 1);              // staging tile q read by its last store
-      mbar_init(smem_u32(&swritten[q]), 4 * NSPLIT);  // staging tile q written (one arrival per epilogue warp)
+    for (int q = 0; q < kBlocks; ++q) {
+      mbar_init(smem_u32(&bfull[q]), 1);
+      mbar_init(smem_u32(&bempty[q]), 4);  // the four epilogue warps of the row
     }
     mbar_init(smem_u32(&done), 1);
     s_stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // weights (all threads), resident for the kernel's lifetime
-  for (int q = tid; q < 9 * NOUT * KC; q += kWsThreads) {
-    const int t = q / (NOUT * KC), r = q % (NOUT * KC), n = r / KC, c = r % KC;
-    cp_async16(Wsm + (uint32_t)(t * NOUT * CIN * 2 + ((n / 8) * KC + c) * 128 + (n % 8) * 16),
-               w + ((long long)t * NOUT + n) * CIN + c * 8, true);
+  // weights, resident for the kernel's lifetime: for column tap dx the B
+  // operand is 3 BW rows, row t BW + n = tap (dy = t - 1, dx) output channel
+  // n (zero for n >= NOUT)
+  for (int q = tid; q < 9 * BW * KC; q += kRowsThreads) {
+    const int dx = q / (3 * BW * KC), r = q % (3 * BW * KC), rr = r / KC, c = r % KC;
+    const int tg = rr / BW, n = rr % BW;
+    const bool ok = n < NOUT;
+    cp_async16(Wsm + (uint32_t)(dx * 3 * WT_BYTES + ((rr / 8) * KC + c) * 128 + (rr % 8) * 16),
+               ok ? (const void *)(w + ((long long)(tg * 3 + dx) * NOUT + n) * CIN + c * 8) : (const void *)w, ok);
   }
-  for (int q = tid; q < NOUT; q += kWsThreads) s_bias[q] = mode == 2 ? 0.f : bias[q];
+  for (int q = tid; q < NOUT; q += kRowsThreads) s_bias[q] = mode == 2 ? 0.f : bias[q];
   cp_async_wait_all();
   fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-
-  struct Pos {
-    int tx, gr, y;
-  };
-  auto advance = [&](Pos a) {
-    ++a.gr;
-    if (++a.y == H) a.y = 0;
-    if (a.gr == (int)NR) {
-      a.gr = 0;
-      a.y = 0;
-      ++a.tx;
-    }
-    return a;
-  };
-  auto row_used = [&](const Pos &a, int dy) { return a.y + dy >= 0 && a.y + dy < H; };
-  Pos first{0, 0, 0};
-  if (t0 < t1) {
-    first.tx = (int)(t0 / NR);
-    first.gr = (int)(t0 % NR);
-    first.y = first.gr % H;
-  }
   auto stop = [&]() {
     s_stop = 1;
     atomicExch(err, 1);
   };
+  RowRun run;
 
-  if (warp >= 8 && warp < 8 + kLoadWarps) {
-    // ---------------------------------------------------------------- loads
-    const int lt = tid - 8 * 32;  // load thread 0 .. 32 * kLoadWarps - 1
-    int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
-    for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
-    Pos a = first;
-    for (long long tile = t0; tile < t1 && !s_stop; ++tile, a = advance(a)) {
-      for (int dy = -1; dy <= 1; ++dy) {
-        if (!row_used(a, dy)) continue;
-        const int r = a.gr + dy, s = r % kWsRing;
-        if (tag_row[s] == r && tag_tx[s] == a.tx) continue;
-        // the slot's previous row is free once the MMAs that read it are done
-        if (nload[s] > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((nload[s] - 1) & 1))) {
-          stop();
+  if (warp == 8 && row_tma<CIN>()) {
+    // ----------------------------------------------------- tensor loads
+    if (lane == 0) {
+      int k = 0;
+      long long t = t0;
+      bool ok = true;
+      while (ok && !s_stop && next_run(t, t1, NR, H, run)) {
+        for (int i = run.ilo; i <= run.ihi && !s_stop; ++i, ++k) {
+          const int s = k % kRing, n = k / kRing;
+          if (n > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((n - 1) & 1))) {
+            stop();
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(smem_u32(&tmab[s]), ROW_TX);
+          tma_load3(Ring + (uint32_t)(s * kSlotSW), &tmap_in, 0, run.tx * kM - 1, i, smem_u32(&tmab[s]));
+        }
+      }
+      // no tensor load may still be writing when the CTA exits: the last one
+      // of each slot has landed (the consumer may have stopped early)
+      for (int s = 0; s < kRing && s < k; ++s) {
+        const int n = (k - 1 - s) / kRing;  // uses of slot s: the last is k' = s + n kRing
+        mbar_wait(smem_u32(&tmab[s]), (uint32_t)(n & 1));
+      }
+    }
+  } else if (warp == 9 && row_tma<CIN>()) {
+    // ---------------------------------------- periodic halo, slot release
+    int k = 0;
+    long long t = t0;
+    bool go = true;
+    while (go && !s_stop && next_run(t, t1, NR, H, run)) {
+      const int x0 = run.tx * kM;
+      const bool wl = periodic_x && run.tx == 0, wr = periodic_x && x0 + kM >= W;
+      for (int i = run.ilo; i <= run.ihi && !s_stop; ++i, ++k) {
+        const int s = k % kRing, n = k / kRing;
+        const int ok = __shfl_sync(0xffffffffu, lane == 0 ? (int)mbar_wait(smem_u32(&tmab[s]), (uint32_t)(n & 1)) : 0, 0);
+        if (!ok) {
+          if (lane == 0) stop();
+          go = false;
           break;
         }
-        const int x0 = a.tx * kM;
-        for (int q = lt; q < kHaloW * KC; q += 32 * kLoadWarps) {
+        // the pixel left of x = 0 is x = W - 1; right of x = W - 1 is x = 0
+        const int c = lane & 7;
+        const bool left = lane < 8 && wl, right = lane >= 8 && lane < 16 && wr;
+        if (left || right) {
+          const int u = left ? 0 : W - x0 + 1, xs = left ? W - 1 : 0;
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(in + ((long long)i * W + xs) * CIN) + c);
+          *reinterpret_cast<uint4 *>(sbase + (Ring - base) + s * kSlotSW + u * 128 + ((c ^ (u & 7)) << 4)) = v;
+          fence_async_smem();
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+      }
+    }
+  } else if (warp >= 8 && warp < 12 && !row_tma<CIN>()) {
+    // ------------------------------------------------- cp.async row loads
+    const int lt = tid - 8 * 32;
+    int k = 0;
+    long long t = t0;
+    bool go = true;
+    while (go && !s_stop && next_run(t, t1, NR, H, run)) {
+      const int x0 = run.tx * kM;
+      for (int i = run.ilo; i <= run.ihi && !s_stop; ++i, ++k) {
+        const int s = k % kRing, n = k / kRing;
+        if (n > 0 && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((n - 1) & 1))) {
+          stop();
+          go = false;
+          break;
+        }
+        for (int q = lt; q < kRowPix * KC; q += 32 * 4) {
           const int u = q / KC, c = q % KC;
           int xx = x0 - 1 + u;
           bool ok = true;
@@ -489,79 +561,74 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
               ok = false;
             }
           }
-          const uint32_t dst = ring_sw<CIN>() ? Ring + (uint32_t)(s * kSlotSW + u * 128 + ((c ^ (u & 7)) << 4))
-                                              : Ring + (uint32_t)(c * kPlaneW + s * kRowB + u * 16);
-          cp_async16(dst, ok ? (const void *)(in + ((long long)r * W + xx) * CIN + c * 8) : (const void *)in, ok);
+          cp_async16(Ring + (uint32_t)(c * kPlaneW + s * kRowB + u * 16),
+                     ok ? (const void *)(in + ((long long)i * W + xx) * CIN + c * 8) : (const void *)in, ok);
         }
         cp_async_arrive_noinc(smem_u32(&full[s]));
-        tag_row[s] = r;
-        tag_tx[s] = a.tx;
-        ++nload[s];
       }
     }
     cp_async_wait_all();
-  } else if (warp == 8 + kLoadWarps) {
+  } else if (warp == 12) {
     // ------------------------------------------------------------------ MMA
     if (lane == 0) {
-      constexpr uint32_t idesc = umma_idesc(kM, NOUT, 0, 0);
       const uint64_t adesc0 = umma_desc(Ring, kPlaneW, 128);
       const uint64_t bdesc0 = umma_desc(Wsm, 128, KC * 128);
-      int tag_row[kWsRing], tag_tx[kWsRing], nload[kWsRing];
-      for (int q = 0; q < kWsRing; ++q) tag_row[q] = tag_tx[q] = -1, nload[q] = 0;
-      bool issued = false;
-      Pos a = first;
-      int it = 0;
-      for (long long tile = t0; tile < t1 && !s_stop; ++tile, ++it, a = advance(a)) {
-        const int b = it & 1;
-        bool ok = true;
-        for (int dy = -1; dy <= 1 && ok; ++dy) {
-          if (!row_used(a, dy)) continue;
-          const int r = a.gr + dy, s = r % kWsRing;
-          if (tag_row[s] == r && tag_tx[s] == a.tx) continue;
-          tag_row[s] = r;
-          tag_tx[s] = a.tx;
-          ++nload[s];
-          ok = mbar_spin(smem_u32(&full[s]), (uint32_t)((nload[s] - 1) & 1));
-        }
-        // accumulator b was last drained for tile it - 2
-        if (ok && it >= 2) ok = mbar_spin(smem_u32(&acce[b]), (uint32_t)(((it >> 1) - 1) & 1));
-        if (!ok) {
-          stop();
-          break;
-        }
-        // the rows arrived through cp.async (generic proxy); the MMAs read
-        // them through the async proxy
-        fence_async_smem();
-        tc_fence_after();
-        uint32_t accum = 0;
-        #pragma unroll
-        for (int tp = 0; tp < 9; ++tp) {
-          const int dy = tp / 3 - 1, dx = tp % 3 - 1;
-          if (!row_used(a, dy)) continue;
-          const int s = (a.gr + dy) % kWsRing;
+      int k = 0, qbase = 0;
+      bool issued = false, go = true;
+      long long t = t0;
+      while (go && !s_stop && next_run(t, t1, NR, H, run)) {
+        for (int i = run.ilo; i <= run.ihi; ++i, ++k) {
+          const int y = i % H;
+          // targets: 0 = output i + 1 (tap dy = -1), 1 = output i, 2 = output i - 1
+          const bool v0 = i + 1 <= run.re && y < H - 1, v1 = i >= run.rb && i <= run.re, v2 = i - 1 >= run.rb && y > 0;
+          const int ta = v0 ? 0 : (v1 ? 1 : 2), tb = v2 ? 2 : (v1 ? 1 : 0);
+          const int q0 = qbase + (i + 1 - run.rb);  // output number of target 0 (q of target t: q0 - t)
+          const bool nw1 = y == 0;                  // output i starts here (no row above in its image)
+          bool ok = true;
+          // blocks this row starts: drained of their previous output
+          if (v0 && q0 >= kBlocks) ok = mbar_spin(smem_u32(&bempty[7 - (q0 & 7)]), (uint32_t)(((q0 >> 3) - 1) & 1));
+          if (ok && v1 && nw1 && q0 - 1 >= kBlocks)
+            ok = mbar_spin(smem_u32(&bempty[7 - ((q0 - 1) & 7)]), (uint32_t)((((q0 - 1) >> 3) - 1) & 1));
+          const int s = k % kRing;
+          if (ok) ok = mbar_spin(smem_u32(&full[s]), (uint32_t)((k / kRing) & 1));
+          if (!ok || s_stop) {
+            if (!ok) stop();
+            go = false;
+            break;
+          }
+          fence_async_smem();
+          tc_fence_after();
           #pragma unroll
-          for (int j = 0; j < CIN / 16; ++j) {
-            const uint64_t ad = ring_sw<CIN>()
-                                    ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW + (dx + 1) * 128 + j * 32))
-                                    : adesc0 + (uint64_t)((s * kRowB + (dx + 1) * 16 + 2 * j * kPlaneW) >> 4);
-            const uint64_t bd = bdesc0 + (uint64_t)((tp * NOUT * CIN * 2 + j * 256) >> 4);
-            umma_bf16(tmem + (uint32_t)b * NCOLS, ad, bd, idesc, accum);
-            accum = 1u;
+          for (int dx = 0; dx < 3; ++dx) {
+            #pragma unroll
+            for (int j = 0; j < CIN / 16; ++j) {
+              const bool first = dx == 0 && j == 0;
+              const uint64_t ad = row_tma<CIN>()
+                                      ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW + dx * 128 + j * 32))
+                                      : adesc0 + (uint64_t)((s * kRowB + dx * 16 + 2 * j * kPlaneW) >> 4);
+              int sa = ta;
+              for (int tt = ta; tt <= tb; ++tt) {
+                // a run of targets ends where the block ring wraps or (first
+                // step) where a started block meets an accumulating one
+                const bool nw_t = tt == 0 || (tt == 1 && nw1), nw_n = tt + 1 == 1 && nw1;
+                const bool brk = tt == tb || ((q0 - tt) & 7) == 0 || (first && nw_t != nw_n);
+                if (!brk) continue;
+                const int nt = tt - sa + 1;
+                const bool nw_a = sa == 0 || (sa == 1 && nw1);
+                const uint32_t d = tmem + (uint32_t)((7 - ((q0 - sa) & 7)) * BW);
+                const uint64_t bd = bdesc0 + (uint64_t)(((dx * 3 + sa) * WT_BYTES + j * 256) >> 4);
+                const uint32_t idesc = umma_idesc(kM, nt * BW, 0, 0);
+                umma_bf16(d, ad, bd, idesc, (first && nw_a) ? 0u : 1u);
+                sa = tt + 1;
+              }
+            }
           }
+          issued = true;
+          umma_commit(smem_u32(&empty[s]));
+          if (v2) umma_commit(smem_u32(&bfull[7 - ((q0 - 2) & 7)]));
+          if (v1 && y == H - 1) umma_commit(smem_u32(&bfull[7 - ((q0 - 1) & 7)]));
         }
-        umma_commit(smem_u32(&accf[b]));
-        issued = true;
-        // release the rows the next tile does not read
-        if (tile + 1 < t1) {
-          const Pos n = advance(a);
-          for (int dy = -1; dy <= 1; ++dy) {
-            if (!row_used(a, dy)) continue;
-            const int r = a.gr + dy;
-            const int ndy = r - n.gr;
-            const bool kept = n.tx == a.tx && ndy >= -1 && ndy <= 1 && row_used(n, ndy);
-            if (!kept) umma_commit(smem_u32(&empty[r % kWsRing]));
-          }
-        }
+        qbase += run.re - run.rb + 1;
       }
       // every MMA issued has completed before tensor memory is freed
       if (issued) {
@@ -569,113 +636,103 @@ __global__ void __launch_bounds__(kWsThreads) k_conv_ws(const __nv_bfloat16 *__r
         if (!mbar_wait(smem_u32(&done), 0)) atomicExch(err, 1);
       }
     }
-  } else {
+  } else if (warp < 8) {
     // ------------------------------------------------------------- epilogue
-    const int quarter = warp & 3, half = warp >> 2;  // lane quarter, column half
+    const int quarter = warp & 3, par = warp >> 2;
     const int m = quarter * 32 + lane;
-    const int c_lo = half * CPW;                       // this warp's first column
-    Pos a = first;
-    int it = 0;
-    for (long long tile = t0; tile < t1 && !s_stop && half < NSPLIT; ++tile, ++it, a = advance(a)) {
-      const int b = it & 1;
-      const int x0 = a.tx * kM, x = x0 + m;
-      const long long p = (long long)a.gr * W + x;
-      // the ReLU mask of this pixel's columns, fetched before the wait
-      uint4 am[CPW / 8];
-      if (mode == 2) {
-        #pragma unroll
-        for (int c = 0; c < CPW / 8; ++c)
-          am[c] = x < W ? __ldg(reinterpret_cast<const uint4 *>(aux + p * NOUT + c_lo) + c) : make_uint4(0, 0, 0, 0);
-      }
-      const bool ok = mbar_wait(smem_u32(&accf[b]), (uint32_t)((it >> 1) & 1));
-      if (!ok) stop();
-      if (__any_sync(0xffffffffu, !ok)) break;
-      tc_fence_after();
-      uint32_t r[CPW];
-      const uint32_t lane_addr = tmem + (uint32_t)b * NCOLS + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c_lo;
-      #pragma unroll
-      for (int c0 = 0; c0 < CPW; c0 += 16) tmem_ld16_nowait(lane_addr + c0, r + c0);
-      tmem_ld_wait();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
-      if (mode == 1) {
-        if (x < W && c_lo < nstore) {
-          float *o = (float *)out + p * nstore;
-          if (nstore == 4 && c_lo == 0) {
-            *reinterpret_cast<float4 *>(o) =
-                make_float4(__uint_as_float(r[0]) + s_bias[0], __uint_as_float(r[1]) + s_bias[1],
-                            __uint_as_float(r[2]) + s_bias[2], __uint_as_float(r[3]) + s_bias[3]);
-          } else {
-            #pragma unroll
-            for (int q = 0; q < CPW; ++q)
-              if (c_lo + q < nstore) o[c_lo + q] = __uint_as_float(r[q]) + s_bias[c_lo + q];
-          }
-        }
-        continue;
-      }
-      uint32_t pk[CPW / 2];
-      #pragma unroll
-      for (int q = 0; q < CPW / 2; ++q) {
-        const float v0 = __uint_as_float(r[2 * q]), v1 = __uint_as_float(r[2 * q + 1]);
-        float lo, hi;
-        if (mode == 0) {
-          lo = fmaxf(v0 + s_bias[c_lo + 2 * q], 0.f);
-          hi = fmaxf(v1 + s_bias[c_lo + 2 * q + 1], 0.f);
-        } else {
-          const uint32_t aw = (&am[q / 4].x)[q % 4];
-          const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
-          lo = __low2float(a2) > 0.f ? v0 : 0.f;
-          hi = __high2float(a2) > 0.f ? v1 : 0.f;
-        }
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(lo, hi);
-        pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
-      }
-      if (!tma) {
-        if (x < W) {
-          uint4 *o = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + p * NOUT + c_lo);
+    const uint32_t stg = Stg + (uint32_t)(warp * STG);
+    uint8_t *const stg_p = sbase + warp * STG;
+    int q = 0;
+    bool go = true;
+    long long t = t0;
+    while (go && !s_stop && next_run(t, t1, NR, H, run)) {
+      const int x0 = run.tx * kM, x = x0 + m;
+      for (int o = run.rb; o <= run.re; ++o, ++q) {
+        if ((q & 1) != par) continue;
+        const int b = 7 - (q & 7);
+        const long long p = (long long)o * W + x;
+        uint4 am[NOUT / 8];  // the ReLU mask of this pixel, fetched before the wait
+        if (mode == 2) {
           #pragma unroll
-          for (int c = 0; c < CPW / 8; ++c) o[c] = make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+          for (int c = 0; c < NOUT / 8; ++c)
+            am[c] = x < W ? __ldg(reinterpret_cast<const uint4 *>(aux + p * NOUT) + c) : make_uint4(0, 0, 0, 0);
         }
-        continue;
-      }
-      // staging tile it & 1: the store issued from it two tiles ago has read
-      // it (thread 0 issues every store, so it is the one that can tell)
-      const int sb = it & 1;
-      if (it >= 2) {
-        if (tid == 0) {
-          bulk_wait_read1();
-          mbar_arrive(smem_u32(&sfree[sb]));
-        }
-        if (!mbar_wait(smem_u32(&sfree[sb]), (uint32_t)(((it >> 1) - 1) & 1))) {
-          stop();
+        const bool ok = mbar_wait(smem_u32(&bfull[b]), (uint32_t)((q >> 3) & 1));
+        if (!ok) stop();
+        if (__any_sync(0xffffffffu, !ok)) {
+          go = false;
           break;
         }
-      }
-      uint8_t *row = stg_p + sb * STG + m * 128;
-      #pragma unroll
-      for (int c = 0; c < CPW / 8; ++c) {  // 16-byte chunk cc of the pixel's 128 bytes, 128-byte swizzle
-        const int cc = c_lo / 8 + c;
-        *reinterpret_cast<uint4 *>(row + ((cc ^ (m & 7)) << 4)) =
-            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
-      }
-      fence_async_smem();  // this thread's staging writes, ordered before the TMA store reads them
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&swritten[sb]));
-      if (tid == 0) {
-        if (!mbar_wait(smem_u32(&swritten[sb]), (uint32_t)((it >> 1) & 1))) {
-          stop();
-          break;
+        tc_fence_after();
+        uint32_t r[NOUT];
+        const uint32_t lane_addr = tmem + (uint32_t)(b * BW) + ((uint32_t)(quarter * 32) << 16);
+        #pragma unroll
+        for (int c0 = 0; c0 < NOUT; c0 += 16) tmem_ld16_nowait(lane_addr + c0, r + c0);
+        tmem_ld_wait();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&bempty[b]));
+        if (mode == 1) {
+          if (x < W) {
+            float *o4 = (float *)out + p * nstore;
+            if (nstore == 4) {
+              *reinterpret_cast<float4 *>(o4) =
+                  make_float4(__uint_as_float(r[0]) + s_bias[0], __uint_as_float(r[1]) + s_bias[1],
+                              __uint_as_float(r[2]) + s_bias[2], __uint_as_float(r[3]) + s_bias[3]);
+            } else {
+              #pragma unroll
+              for (int c = 0; c < NOUT; ++c)
+                if (c < nstore) o4[c] = __uint_as_float(r[c]) + s_bias[c];
+            }
+          }
+          continue;
         }
-        tma_store3(&tmap, Stg + (uint32_t)(sb * STG), 0, x0, a.gr);
-        bulk_commit();
+        uint32_t pk[NOUT / 2];
+        #pragma unroll
+        for (int c = 0; c < NOUT / 2; ++c) {
+          const float a0 = __uint_as_float(r[2 * c]), a1 = __uint_as_float(r[2 * c + 1]);
+          float lo, hi;
+          if (mode == 0) {
+            lo = fmaxf(a0 + s_bias[2 * c], 0.f);
+            hi = fmaxf(a1 + s_bias[2 * c + 1], 0.f);
+          } else {
+            const uint32_t aw = (&am[c / 4].x)[c % 4];
+            const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
+            lo = __low2float(a2) > 0.f ? a0 : 0.f;
+            hi = __high2float(a2) > 0.f ? a1 : 0.f;
+          }
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(lo, hi);
+          pk[c] = *reinterpret_cast<const uint32_t *>(&b2);
+        }
+        if (!tma_out) {
+          if (x < W) {
+            uint4 *o16 = reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + p * NOUT);
+            #pragma unroll
+            for (int c = 0; c < NOUT / 8; ++c) o16[c] = make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+          }
+          continue;
+        }
+        // this warp's previous store has read its staging tile
+        if (lane == 0) bulk_wait_read0();
+        __syncwarp();
+        uint8_t *row = stg_p + lane * 128;
+        #pragma unroll
+        for (int c = 0; c < NOUT / 8; ++c)  // 16-byte chunk c of the pixel's 128 bytes, 128-byte swizzle
+          *reinterpret_cast<uint4 *>(row + ((c ^ (lane & 7)) << 4)) =
+              make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+        fence_async_smem();  // the staging writes, ordered before the TMA store reads them
+        __syncwarp();
+        if (lane == 0 && x0 + quarter * 32 < W) {
+          tma_store3(&tmap_out, stg, 0, x0 + quarter * 32, o);
+          bulk_commit();
+        }
       }
     }
-    if (tid == 0) bulk_wait_all();
+    if (lane == 0) bulk_wait_all();
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 2 * NCOLS);
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
 
 // ----------------------------------------------------------------------------
@@ -794,8 +851,8 @@ template <int CIN, int NOUT>
 size_t wgrad_smem() { return smem_floor<NOUT>(2 * (size_t)(kM * 64 * 2 + NOUT * 64 * 2)); }
 
 template <int CIN, int NOUT>
-size_t ws_smem() {
-  return 1024 + (ws_tma<CIN, NOUT>() ? 2 * (size_t)kM * NOUT * 2 : 0) + (size_t)9 * NOUT * CIN * 2 +
+size_t rows_smem() {
+  return 1024 + (store_tma<NOUT>() ? 8 * (size_t)32 * NOUT * 2 : 0) + (size_t)9 * blk_w<NOUT>() * CIN * 2 +
          (size_t)ring_bytes<CIN>();  // 64 -> 64: 1 + 32 + 72 + 102 KB
 }
 
@@ -813,41 +870,50 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// [image rows][W][C] BF16 activations as a 3-D tensor map with a box of
+// box_w pixels x C channels, 128-byte swizzle
+bool act_tensor_map(CUtensorMap *tm, const void *p, int C, int W, int NR, int box_w) {
+  auto enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)p & 15u)) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)NR};
+  const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2};
+  const cuuint32_t box[3] = {(cuuint32_t)C, (cuuint32_t)box_w, 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(p), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int CIN, int NOUT>
-cudaError_t conv_ws_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
-                           const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x, int mode,
-                           int nstore, int *err, cudaStream_t s) {
-  const size_t sm = ws_smem<CIN, NOUT>();
-  cudaError_t e = cudaFuncSetAttribute(k_conv_ws<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+cudaError_t conv_rows_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                             const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x,
+                             int mode, int nstore, int *err, cudaStream_t s) {
+  const size_t sm = rows_smem<CIN, NOUT>();
+  cudaError_t e = cudaFuncSetAttribute(k_conv_rows<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const long long hw = (long long)H * W;
-  const int nimg = (int)(npix / hw);
-  const long long NR = (long long)nimg * H;
-  const long long ntiles = NR * ((W + kM - 1) / kM);
-  // output tensor map: [image rows][W][NOUT] BF16, box = one tile (128 pixels
-  // x 64 channels), 128-byte swizzle; pixels past W in a tile are not stored
-  CUtensorMap tm;
-  memset(&tm, 0, sizeof tm);
-  if (ws_tma<CIN, NOUT>() && mode != 1) {
-    auto enc = tensor_map_encoder();
-    if (!enc || NR > 0x7fffffffLL || ((uintptr_t)out & 15u)) return cudaErrorInvalidValue;
-    const cuuint64_t dims[3] = {(cuuint64_t)NOUT, (cuuint64_t)W, (cuuint64_t)NR};
-    const cuuint64_t strides[2] = {(cuuint64_t)NOUT * 2, (cuuint64_t)W * NOUT * 2};
-    const cuuint32_t box[3] = {(cuuint32_t)NOUT, (cuuint32_t)kM, 1u};
-    const cuuint32_t estr[3] = {1u, 1u, 1u};
-    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, out, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return cudaErrorInvalidValue;
-  }
+  const long long NRl = npix / hw;
+  if (NRl * H > 0x7fffffffLL) return cudaErrorInvalidValue;
+  const int nimg = (int)NRl, NR = nimg * H;
+  const long long ntiles = (long long)NR * ((W + kM - 1) / kM);
+  // input rows: one box = the 130 pixels of a tile and its halo; output:
+  // one box = an epilogue warp's 32 pixels; pixels past W are zero-filled
+  // (loads) or not written (stores)
+  CUtensorMap tin, tout;
+  memset(&tin, 0, sizeof tin);
+  memset(&tout, 0, sizeof tout);
+  if (row_tma<CIN>() && !act_tensor_map(&tin, in, CIN, W, NR, kRowPix)) return cudaErrorInvalidValue;
+  if (store_tma<NOUT>() && mode != 1 && !act_tensor_map(&tout, out, NOUT, W, NR, 32)) return cudaErrorInvalidValue;
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_ws<CIN, NOUT>, kWsThreads, sm);
-  const int tmem_cap = 512 / (2 * (NOUT < 32 ? 32 : NOUT));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_rows<CIN, NOUT>, kRowsThreads, sm);
+  const int tmem_cap = 512 / (kBlocks * blk_w<NOUT>());
   per = per < 1 ? 1 : (per > tmem_cap ? tmem_cap : per);
   const long long grid = ntiles < (long long)nsm * per ? ntiles : (long long)nsm * per;
-  k_conv_ws<CIN, NOUT><<<(unsigned)grid, kWsThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x, mode,
-                                                               nstore, err, tm);
+  if (grid < 1) return cudaSuccess;
+  k_conv_rows<CIN, NOUT><<<(unsigned)grid, kRowsThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x,
+                                                                   mode, nstore, err, tin, tout);
   return cudaGetLastError();
 }
 
@@ -855,9 +921,9 @@ template <int CIN, int NOUT>
 cudaError_t conv_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, const __nv_bfloat16 *aux,
                         void *out, long long npix, int H, int W, int periodic_x, int mode, int nstore, int *err,
                         cudaStream_t s) {
-  // whole images: the persistent warp-specialised form
+  // whole images: the persistent row-streaming form
   if (npix % ((long long)H * W) == 0)
-    return conv_ws_launch<CIN, NOUT>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
+    return conv_rows_launch<CIN, NOUT>(in, w, bias, aux, out, npix, H, W, periodic_x, mode, nstore, err, s);
   const size_t sm = conv_smem<CIN, NOUT>();
   cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
