@@ -596,6 +596,33 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
             go = false;
             break;
           }
+          // the row's MMA runs: target t starts one where the row before it
+          // is invalid or not adjacent in tensor memory (ring wrap, or on the
+          // first step a started block next to an accumulating one); worked
+          // out once per row so that each MMA costs two adds and the issue
+          const bool nw[3] = {true, nw1, false};
+          const bool v[3] = {v0, v1, v2};
+          bool stF[3], stR[3];
+          uint32_t col[3], idF[3], idR[3], accF[3];
+          #pragma unroll
+          for (int tt = 0; tt < 3; ++tt) {
+            col[tt] = tmem + (uint32_t)((7 - ((q0 - tt) & 7)) * BW);
+            const bool adj = tt > 0 && v[tt - 1] && ((q0 - tt + 1) & 7) != 0;  // joins target tt - 1
+            stR[tt] = v[tt] && !adj;
+            stF[tt] = v[tt] && !(adj && nw[tt] == nw[tt - (tt > 0)]);
+            int eR = tt, eF = tt;  // last target of the run starting at tt
+            #pragma unroll
+            for (int u = tt + 1; u < 3; ++u) {
+              const bool jn = v[u] && ((q0 - u + 1) & 7) != 0;
+              if (eR == u - 1 && jn) eR = u;
+              if (eF == u - 1 && jn && nw[u] == nw[tt]) eF = u;
+            }
+            idR[tt] = umma_idesc(kM, (eR - tt + 1) * BW, 0, 0);
+            idF[tt] = umma_idesc(kM, (eF - tt + 1) * BW, 0, 0);
+            accF[tt] = nw[tt] ? 0u : 1u;
+          }
+          const uint64_t arow = row_tma<CIN>() ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW))
+                                               : adesc0 + (uint64_t)((s * kRowB) >> 4);
           fence_async_smem();
           tc_fence_after();
           #pragma unroll
@@ -603,23 +630,14 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
             #pragma unroll
             for (int j = 0; j < CIN / 16; ++j) {
               const bool first = dx == 0 && j == 0;
-              const uint64_t ad = row_tma<CIN>()
-                                      ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW + dx * 128 + j * 32))
-                                      : adesc0 + (uint64_t)((s * kRowB + dx * 16 + 2 * j * kPlaneW) >> 4);
-              int sa = ta;
-              for (int tt = ta; tt <= tb; ++tt) {
-                // a run of targets ends where the block ring wraps or (first
-                // step) where a started block meets an accumulating one
-                const bool nw_t = tt == 0 || (tt == 1 && nw1), nw_n = tt + 1 == 1 && nw1;
-                const bool brk = tt == tb || ((q0 - tt) & 7) == 0 || (first && nw_t != nw_n);
-                if (!brk) continue;
-                const int nt = tt - sa + 1;
-                const bool nw_a = sa == 0 || (sa == 1 && nw1);
-                const uint32_t d = tmem + (uint32_t)((7 - ((q0 - sa) & 7)) * BW);
-                const uint64_t bd = bdesc0 + (uint64_t)(((dx * 3 + sa) * WT_BYTES + j * 256) >> 4);
-                const uint32_t idesc = umma_idesc(kM, nt * BW, 0, 0);
-                umma_bf16(d, ad, bd, idesc, (first && nw_a) ? 0u : 1u);
-                sa = tt + 1;
+              // A: the row from pixel dx (column tap dx - 1), K step j
+              const uint64_t ad = arow + (uint64_t)(row_tma<CIN>() ? (dx * 128 + j * 32) >> 4 : (dx * 16 + 2 * j * kPlaneW) >> 4);
+              #pragma unroll
+              for (int tt = 0; tt < 3; ++tt) {
+                if (first ? stF[tt] : stR[tt]) {
+                  const uint64_t bd = bdesc0 + (uint64_t)(((dx * 3 + tt) * WT_BYTES + j * 256) >> 4);
+                  umma_bf16(col[tt], ad, bd, first ? idF[tt] : idR[tt], first ? accF[tt] : 1u);
+                }
               }
             }
           }
