@@ -129,6 +129,21 @@ __device__ __forceinline__ bool mbar_spin(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+// one test each of two mbarrier phases, issued together so that their
+// latencies overlap; bit 0 = the first complete, bit 1 = the second
+__device__ __forceinline__ uint32_t mbar_test2(uint32_t mbar0, uint32_t parity0, uint32_t mbar1, uint32_t parity1) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t.reg .b32 a, b;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 q, [%3], %4;\n\t"
+      "selp.b32 a, 1, 0, p;\n\tselp.b32 b, 2, 0, q;\n\tor.b32 %0, a, b;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar0), "r"(parity0), "r"(mbar1), "r"(parity1)
+      : "memory");
+  return done;
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
   const int n = valid ? 16 : 0;  // 0: zero-fill
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
@@ -362,6 +377,21 @@ __host__ __device__ constexpr int blk_w() { return NOUT < 32 ? 32 : NOUT; }
 template <int NOUT>
 __host__ __device__ constexpr bool store_tma() { return NOUT == 64; }
 
+// tcgen05.mma with each descriptor given as its two 32-bit words
+__device__ __forceinline__ void umma_bf16_w(uint32_t tmem_d, uint32_t a_lo, uint32_t a_hi, uint32_t b_lo, uint32_t b_hi,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t.reg .b64 ad, bd;\n\tsetp.ne.b32 p, %6, 0;\n\tmov.b64 ad, {%1, %2};\n\t"
+      "mov.b64 bd, {%3, %4};\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], ad, bd, %5, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(a_lo), "r"(a_hi), "r"(b_lo), "r"(b_hi), "r"(idesc), "r"(accumulate));
+}
+// start-address step (16-byte units) of the A operand of column tap dx, K
+// step j within a ring slot: dx pixels in, K columns j * 16 in
+template <int CIN>
+__host__ __device__ constexpr uint32_t a_step(int dx, int j) {
+  return row_tma<CIN>() ? (uint32_t)(dx * 8 + j * 2) : (uint32_t)(dx + j * (2 * kPlaneW / 16));
+}
+
 __device__ __forceinline__ void cp_async_arrive_noinc(uint32_t mbar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
 }
@@ -415,7 +445,7 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
                                                             int H, int W, int periodic_x, int mode, int nstore,
                                                             int *err, const __grid_constant__ CUtensorMap tmap_in,
                                                             const __grid_constant__ CUtensorMap tmap_out) {
-  constexpr int KC = CIN / 8;
+  constexpr int KC = CIN / 8, KJ = CIN / 16;  // 16-byte chunks, K steps of one pixel
   constexpr int BW = blk_w<NOUT>();
   constexpr int WT_BYTES = BW * CIN * 2;      // one target's weights of one column tap
   constexpr int W_BYTES = 9 * WT_BYTES;       // [column tap][target][BW rows][CIN]
@@ -425,7 +455,7 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
   static_assert(!row_tma<CIN>() || (W_BYTES % 1024 == 0 && STG % 1024 == 0), "swizzled slots need 1024-byte alignment");
   static_assert(3 * BW <= 256, "N of one MMA");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ float s_bias[NOUT];
+  __shared__ __align__(16) float s_bias[NOUT];
   __shared__ __align__(8) uint64_t full[kRing], tmab[kRing], empty[kRing], bfull[kBlocks], bempty[kBlocks], done;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int s_stop;
@@ -571,14 +601,28 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
   } else if (warp == 12) {
     // ------------------------------------------------------------------ MMA
     if (lane == 0) {
-      const uint64_t adesc0 = umma_desc(Ring, kPlaneW, 128);
+      // descriptors as a 32-bit low word (start address, leading byte
+      // offset) over a fixed high word: the offsets added below stay inside
+      // the 14-bit start field (shared-memory addresses < 256 KB)
+      const uint64_t adesc0 = row_tma<CIN>() ? umma_desc_sw128(Ring) : umma_desc(Ring, kPlaneW, 128);
       const uint64_t bdesc0 = umma_desc(Wsm, 128, KC * 128);
-      int k = 0, qbase = 0;
+      const uint32_t a_hi = (uint32_t)(adesc0 >> 32), b_hi = (uint32_t)(bdesc0 >> 32);
+      const uint32_t a_lo0 = (uint32_t)adesc0, b_lo0 = (uint32_t)bdesc0;
+      constexpr uint32_t SLOT16 = (row_tma<CIN>() ? kSlotSW : kRowB) / 16;  // one ring slot, 16-byte units
+      constexpr uint32_t WT16 = WT_BYTES / 16;
+      int qbase = 0, s = 0;  // s: ring slot of the current row
+      uint32_t ph = 0;       // parity of slot s's current fill
+      // the next row's slot and first block, tested right after this row's
+      // MMAs are issued, while they run (a test took ~400 cycles while the
+      // MMAs read shared memory; two in a row at the top of each row left
+      // the tensor pipe idle)
+      uint32_t pre_ok = 0;
+      bool pre = false;
       bool issued = false, go = true;
       long long t = t0;
       while (go && !s_stop && next_run(t, t1, NR, H, run)) {
-        for (int i = run.ilo; i <= run.ihi; ++i, ++k) {
-          const int y = i % H;
+        int y = run.ilo % H;  // image row of input row i
+        for (int i = run.ilo; i <= run.ihi; ++i) {
           // targets: 0 = output i + 1 (tap dy = -1), 1 = output i, 2 = output i - 1
           const bool v0 = i + 1 <= run.re && y < H - 1, v1 = i >= run.rb && i <= run.re, v2 = i - 1 >= run.rb && y > 0;
           const int ta = v0 ? 0 : (v1 ? 1 : 2), tb = v2 ? 2 : (v1 ? 1 : 0);
@@ -586,65 +630,97 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
           const bool nw1 = y == 0;                  // output i starts here (no row above in its image)
           bool ok = true;
           // blocks this row starts: drained of their previous output
-          if (v0 && q0 >= kBlocks) ok = mbar_spin(smem_u32(&bempty[7 - (q0 & 7)]), (uint32_t)(((q0 >> 3) - 1) & 1));
+          if (v0 && q0 >= kBlocks && !(pre && (pre_ok & 2u)))
+            ok = mbar_spin(smem_u32(&bempty[7 - (q0 & 7)]), (uint32_t)(((q0 >> 3) - 1) & 1));
           if (ok && v1 && nw1 && q0 - 1 >= kBlocks)
             ok = mbar_spin(smem_u32(&bempty[7 - ((q0 - 1) & 7)]), (uint32_t)((((q0 - 1) >> 3) - 1) & 1));
-          const int s = k % kRing;
-          if (ok) ok = mbar_spin(smem_u32(&full[s]), (uint32_t)((k / kRing) & 1));
+          if (ok && !(pre && (pre_ok & 1u))) ok = mbar_spin(smem_u32(&full[s]), ph);
           if (!ok || s_stop) {
             if (!ok) stop();
             go = false;
             break;
           }
-          // the row's MMA runs: target t starts one where the row before it
-          // is invalid or not adjacent in tensor memory (ring wrap, or on the
-          // first step a started block next to an accumulating one); worked
-          // out once per row so that each MMA costs two adds and the issue
-          const bool nw[3] = {true, nw1, false};
-          const bool v[3] = {v0, v1, v2};
-          bool stF[3], stR[3];
-          uint32_t col[3], idF[3], idR[3], accF[3];
-          #pragma unroll
-          for (int tt = 0; tt < 3; ++tt) {
-            col[tt] = tmem + (uint32_t)((7 - ((q0 - tt) & 7)) * BW);
-            const bool adj = tt > 0 && v[tt - 1] && ((q0 - tt + 1) & 7) != 0;  // joins target tt - 1
-            stR[tt] = v[tt] && !adj;
-            stF[tt] = v[tt] && !(adj && nw[tt] == nw[tt - (tt > 0)]);
-            int eR = tt, eF = tt;  // last target of the run starting at tt
-            #pragma unroll
-            for (int u = tt + 1; u < 3; ++u) {
-              const bool jn = v[u] && ((q0 - u + 1) & 7) != 0;
-              if (eR == u - 1 && jn) eR = u;
-              if (eF == u - 1 && jn && nw[u] == nw[tt]) eF = u;
-            }
-            idR[tt] = umma_idesc(kM, (eR - tt + 1) * BW, 0, 0);
-            idF[tt] = umma_idesc(kM, (eF - tt + 1) * BW, 0, 0);
-            accF[tt] = nw[tt] ? 0u : 1u;
-          }
-          const uint64_t arow = row_tma<CIN>() ? umma_desc_sw128(Ring + (uint32_t)(s * kSlotSW))
-                                               : adesc0 + (uint64_t)((s * kRowB) >> 4);
+          // The row's MMAs.  A run of adjacent targets shares one MMA; target
+          // t starts a new run where target t - 1 is invalid or its block is
+          // not adjacent (the ring wraps between them) and, on the first
+          // step, where a block that starts here meets one that accumulates.
+          // The issuing thread is this kernel's limit: with the runs worked
+          // out in the loop, runtime branches and 64-bit descriptor
+          // arithmetic per MMA, it issued one MMA per ~235 cycles with every
+          // other role switched off; the straight-line sequences below add
+          // compile-time offsets to 32-bit words.
+          // the other steps: one run from ta, or two where the ring wraps
+          // between targets 0 and 1 or 1 and 2
+          const int r2 = (ta == 0 && tb >= 1 && (q0 & 7) == 0) ? 1 : ((ta <= 1 && tb == 2 && ((q0 - 1) & 7) == 0) ? 2 : -1);
+          const uint32_t a_lo = a_lo0 + (uint32_t)s * SLOT16;
           fence_async_smem();
           tc_fence_after();
-          #pragma unroll
-          for (int dx = 0; dx < 3; ++dx) {
+          if (ta == 0 && tb == 2 && r2 < 0 && !nw1) {
+            // the common row: outputs i + 1, i, i - 1 in adjacent blocks, only
+            // output i + 1 starting: step 0 = [i + 1] (starts its block) and
+            // [i, i - 1]; the other steps one MMA over all three
+            const uint32_t c0 = tmem + (uint32_t)((7 - (q0 & 7)) * BW);
+            umma_bf16_w(c0, a_lo, a_hi, b_lo0, b_hi, umma_idesc(kM, BW, 0, 0), 0u);
+            umma_bf16_w(c0 + BW, a_lo, a_hi, b_lo0 + WT16, b_hi, umma_idesc(kM, 2 * BW, 0, 0), 1u);
             #pragma unroll
-            for (int j = 0; j < CIN / 16; ++j) {
-              const bool first = dx == 0 && j == 0;
-              // A: the row from pixel dx (column tap dx - 1), K step j
-              const uint64_t ad = arow + (uint64_t)(row_tma<CIN>() ? (dx * 128 + j * 32) >> 4 : (dx * 16 + 2 * j * kPlaneW) >> 4);
+            for (int st = 1; st < 3 * KJ; ++st)
+              umma_bf16_w(c0, a_lo + a_step<CIN>(st / KJ, st % KJ), a_hi,
+                          b_lo0 + (uint32_t)((st / KJ) * 3 * WT16 + (st % KJ) * 16), b_hi, umma_idesc(kM, 3 * BW, 0, 0),
+                          1u);
+          } else {
+            const bool nw[3] = {true, nw1, false};
+            const bool v[3] = {v0, v1, v2};
+            // step 0 (column tap 0, K step 0)
+            #pragma unroll
+            for (int tt = 0; tt < 3; ++tt) {
+              const bool adj = tt > 0 && v[tt - 1] && ((q0 - tt + 1) & 7) != 0;  // joins target tt - 1
+              if (v[tt] && !(adj && nw[tt] == nw[tt - (tt > 0)])) {
+                int e = tt;  // last target of the first-step run starting at tt
+                #pragma unroll
+                for (int u = tt + 1; u < 3; ++u)
+                  if (e == u - 1 && v[u] && ((q0 - u + 1) & 7) != 0 && nw[u] == nw[tt]) e = u;
+                umma_bf16_w(tmem + (uint32_t)((7 - ((q0 - tt) & 7)) * BW), a_lo, a_hi, b_lo0 + (uint32_t)tt * WT16, b_hi,
+                            umma_idesc(kM, (e - tt + 1) * BW, 0, 0), nw[tt] ? 0u : 1u);
+              }
+            }
+            // steps 1 .. 3 KJ - 1: column tap dx = st / KJ, K step j = st % KJ
+            const uint32_t colA = tmem + (uint32_t)((7 - ((q0 - ta) & 7)) * BW);
+            const uint32_t idA = umma_idesc(kM, ((r2 < 0 ? tb : r2 - 1) - ta + 1) * BW, 0, 0);
+            const uint32_t bA = b_lo0 + (uint32_t)ta * WT16;
+            if (r2 < 0) {
               #pragma unroll
-              for (int tt = 0; tt < 3; ++tt) {
-                if (first ? stF[tt] : stR[tt]) {
-                  const uint64_t bd = bdesc0 + (uint64_t)(((dx * 3 + tt) * WT_BYTES + j * 256) >> 4);
-                  umma_bf16(col[tt], ad, bd, first ? idF[tt] : idR[tt], first ? accF[tt] : 1u);
-                }
+              for (int st = 1; st < 3 * KJ; ++st)
+                umma_bf16_w(colA, a_lo + a_step<CIN>(st / KJ, st % KJ), a_hi,
+                            bA + (uint32_t)((st / KJ) * 3 * WT16 + (st % KJ) * 16), b_hi, idA, 1u);
+            } else {
+              const uint32_t colB = tmem + (uint32_t)((7 - ((q0 - r2) & 7)) * BW);
+              const uint32_t idB = umma_idesc(kM, (tb - r2 + 1) * BW, 0, 0);
+              const uint32_t bB = b_lo0 + (uint32_t)r2 * WT16;
+              #pragma unroll
+              for (int st = 1; st < 3 * KJ; ++st) {
+                const uint32_t ad = a_lo + a_step<CIN>(st / KJ, st % KJ);
+                const uint32_t boff = (uint32_t)((st / KJ) * 3 * WT16 + (st % KJ) * 16);
+                umma_bf16_w(colA, ad, a_hi, bA + boff, b_hi, idA, 1u);
+                umma_bf16_w(colB, ad, a_hi, bB + boff, b_hi, idB, 1u);
               }
             }
           }
+          // row i + 1 of the same run: its slot, and the block of its output
+          // i + 2 (output q0 + 1), whose drain it needs (the block's first
+          // use needs none: a test of the phase before its first reads 1)
+          pre = i + 1 <= run.ihi;
+          if (pre)
+            pre_ok = mbar_test2(smem_u32(&full[s + 1 == kRing ? 0 : s + 1]), s + 1 == kRing ? ph ^ 1u : ph,
+                                smem_u32(&bempty[7 - ((q0 + 1) & 7)]), (uint32_t)((((q0 + 1) >> 3) - 1) & 1));
           issued = true;
           umma_commit(smem_u32(&empty[s]));
           if (v2) umma_commit(smem_u32(&bfull[7 - ((q0 - 2) & 7)]));
           if (v1 && y == H - 1) umma_commit(smem_u32(&bfull[7 - ((q0 - 1) & 7)]));
+          if (++y == H) y = 0;
+          if (++s == kRing) {
+            s = 0;
+            ph ^= 1u;
+          }
         }
         qbase += run.re - run.rb + 1;
       }
@@ -711,8 +787,10 @@ __global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 
           const float a0 = __uint_as_float(r[2 * c]), a1 = __uint_as_float(r[2 * c + 1]);
           float lo, hi;
           if (mode == 0) {
-            lo = fmaxf(a0 + s_bias[2 * c], 0.f);
-            hi = fmaxf(a1 + s_bias[2 * c + 1], 0.f);
+            // bias four channels per shared-memory load
+            const float4 b4 = reinterpret_cast<const float4 *>(s_bias)[c / 2];
+            lo = fmaxf(a0 + ((c & 1) ? b4.z : b4.x), 0.f);
+            hi = fmaxf(a1 + ((c & 1) ? b4.w : b4.y), 0.f);
           } else {
             const uint32_t aw = (&am[c / 4].x)[c % 4];
             const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
