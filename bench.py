@@ -539,6 +539,27 @@ def run_closure_leg(args, case, plain_ms):
             "note": "cost with random weights; accuracy: pcom_b200.closure (configuration 5)"}
 
 
+def run_global025_leg(args, steps: int = 8):
+    """The 1440x640x30 0.25-degree case (dtbc 1200 s, dtbt 20 s), FP64 and
+    mixed: time per step (CUDA events, device-resident, ~10 GB of state) and
+    the per-kernel algorithmic GB/s of a second pass with kernel events."""
+    from pcom_b200.roofline import kernel_table
+    from pcom_b200.synth import make_case
+
+    case = make_case("global025")
+    out = {"grid": [case["glo_ni"], case["glo_nj"], case["nk"]], "dtbc": case["dtbc"], "dtbt": case["dtbt"],
+           "steps": steps}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        t = kernel_table(case, mixed, steps)
+        ms = t["ms_per_step"]
+        top = dict(list(t["kernels"].items())[:6])
+        out[name] = {"ms_per_step": ms, "value": round(sypd(ms / 1000.0, case["dtbc"]), 2), "unit": "SYPD",
+                     "kernels": {k: {"us": v["us_per_launch"], "GB_s": v["GB_s"], "frac": v["frac_of_peak"]}
+                                 for k, v in top.items()},
+                     "peak_GB_s": t["peak_GB_s"], "peak_source": t["peak_source"]}
+    return out
+
+
 def ensemble_cases(members: int, basins: int, member_case: str = "box"):
     """Members of one case (default the 128x64x20 1-degree box) with seeded
     N(0, 0.05 K) perturbations of T (seeds 1..members), and idealized basins

@@ -438,7 +438,7 @@ __device__ __forceinline__ bool next_run(long long &t, long long t1, int NR, int
 }
 
 template <int CIN, int NOUT>
-__global__ void __launch_bounds__(kRowsThreads) k_conv_rows(const __nv_bfloat16 *__restrict__ in,
+__global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat16 *__restrict__ in,
                                                             const __nv_bfloat16 *__restrict__ w,
                                                             const float *__restrict__ bias,
                                                             const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
