@@ -437,14 +437,21 @@ __device__ __forceinline__ bool next_run(long long &t, long long t1, int NR, int
   return true;
 }
 
-template <int CIN, int NOUT>
+// (in the MODE 1 instantiation the BF16 epilogue after its `continue` is
+// unreachable by design)
+#pragma nv_diag_suppress 128
+// MODE (compile time, so that each epilogue holds only its own registers):
+// 0 = + bias, ReLU, BF16 out; 1 = + bias, FP32 out, first nstore channels;
+// 2 = ReLU mask from aux, BF16 out
+template <int CIN, int NOUT, int MODE>
 __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat16 *__restrict__ in,
                                                             const __nv_bfloat16 *__restrict__ w,
                                                             const float *__restrict__ bias,
                                                             const __nv_bfloat16 *__restrict__ aux, void *out, int nimg,
-                                                            int H, int W, int periodic_x, int mode, int nstore,
-                                                            int *err, const __grid_constant__ CUtensorMap tmap_in,
+                                                            int H, int W, int periodic_x, int nstore, int *err,
+                                                            const __grid_constant__ CUtensorMap tmap_in,
                                                             const __grid_constant__ CUtensorMap tmap_out) {
+  constexpr int mode = MODE;
   constexpr int KC = CIN / 8, KJ = CIN / 16;  // 16-byte chunks, K steps of one pixel
   constexpr int BW = blk_w<NOUT>();
   constexpr int WT_BYTES = BW * CIN * 2;      // one target's weights of one column tap
@@ -734,6 +741,12 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat
     // ------------------------------------------------------------- epilogue
     const int quarter = warp & 3, par = warp >> 2;
     const int m = quarter * 32 + lane;
+    // mode 0: the bias in registers (read from shared memory per row it
+    // took ~1,500 of the ~2,700 cycles of a 64-channel row's conversion
+    // while the MMAs stream their operands)
+    float breg[mode == 0 ? NOUT : 1];
+    #pragma unroll
+    for (int c = 0; c < (mode == 0 ? NOUT : 1); ++c) breg[c] = mode == 0 ? s_bias[c] : 0.f;
     const uint32_t stg = Stg + (uint32_t)(warp * STG);
     uint8_t *const stg_p = sbase + warp * STG;
     int q = 0;
@@ -787,10 +800,8 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat
           const float a0 = __uint_as_float(r[2 * c]), a1 = __uint_as_float(r[2 * c + 1]);
           float lo, hi;
           if (mode == 0) {
-            // bias four channels per shared-memory load
-            const float4 b4 = reinterpret_cast<const float4 *>(s_bias)[c / 2];
-            lo = fmaxf(a0 + ((c & 1) ? b4.z : b4.x), 0.f);
-            hi = fmaxf(a1 + ((c & 1) ? b4.w : b4.y), 0.f);
+            lo = fmaxf(a0 + breg[(2 * c) % (mode == 0 ? NOUT : 1)], 0.f);
+            hi = fmaxf(a1 + breg[(2 * c + 1) % (mode == 0 ? NOUT : 1)], 0.f);
           } else {
             const uint32_t aw = (&am[c / 4].x)[c % 4];
             const __nv_bfloat162 a2 = *reinterpret_cast<const __nv_bfloat162 *>(&aw);
@@ -830,6 +841,7 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
+#pragma nv_diag_default 128
 
 // ----------------------------------------------------------------------------
 // Weight gradient: dw[t][n][c] += sum_p in[src(p, t)][c] g[p][n]
@@ -980,12 +992,14 @@ bool act_tensor_map(CUtensorMap *tm, const void *p, int C, int W, int NR, int bo
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int CIN, int NOUT>
-cudaError_t conv_rows_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
-                             const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x,
-                             int mode, int nstore, int *err, cudaStream_t s) {
+template <int CIN, int NOUT, int MODE>
+cudaError_t conv_rows_launch_m(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                               const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x,
+                               int nstore, int *err, cudaStream_t s) {
+  constexpr int mode = MODE;
   const size_t sm = rows_smem<CIN, NOUT>();
-  cudaError_t e = cudaFuncSetAttribute(k_conv_rows<CIN, NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_conv_rows<CIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const long long hw = (long long)H * W;
   const long long NRl = npix / hw;
@@ -1003,14 +1017,24 @@ cudaError_t conv_rows_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, co
   int dev = 0, nsm = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_rows<CIN, NOUT>, kRowsThreads, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv_rows<CIN, NOUT, MODE>, kRowsThreads, sm);
   const int tmem_cap = 512 / (kBlocks * blk_w<NOUT>());
   per = per < 1 ? 1 : (per > tmem_cap ? tmem_cap : per);
   const long long grid = ntiles < (long long)nsm * per ? ntiles : (long long)nsm * per;
   if (grid < 1) return cudaSuccess;
-  k_conv_rows<CIN, NOUT><<<(unsigned)grid, kRowsThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W, periodic_x,
-                                                                   mode, nstore, err, tin, tout);
+  k_conv_rows<CIN, NOUT, MODE><<<(unsigned)grid, kRowsThreads, sm, s>>>(in, w, bias, aux, out, nimg, H, W,
+                                                                         periodic_x, nstore, err, tin, tout);
   return cudaGetLastError();
+}
+
+template <int CIN, int NOUT>
+cudaError_t conv_rows_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                             const __nv_bfloat16 *aux, void *out, long long npix, int H, int W, int periodic_x,
+                             int mode, int nstore, int *err, cudaStream_t s) {
+  if (mode == 0) return conv_rows_launch_m<CIN, NOUT, 0>(in, w, bias, aux, out, npix, H, W, periodic_x, nstore, err, s);
+  if (mode == 1) return conv_rows_launch_m<CIN, NOUT, 1>(in, w, bias, aux, out, npix, H, W, periodic_x, nstore, err, s);
+  if (mode == 2) return conv_rows_launch_m<CIN, NOUT, 2>(in, w, bias, aux, out, npix, H, W, periodic_x, nstore, err, s);
+  return cudaErrorInvalidValue;
 }
 
 template <int CIN, int NOUT>
