@@ -255,7 +255,8 @@ typedef struct {
 int pcom_gpu_coarsen(pcom_handle *fine, pcom_handle *coarse, int32_t factor);
 /* Network input from the state: BF16 [nk][glo_nj][glo_ni][16] (device),
  * channels (uc, vc, tc, sc, alpha - alpha_ref) normalised by `stats`, zero
- * on land and in channels 5..15. */
+ * on land and in channels 5..15.  x_bf16 must be 16-byte aligned
+ * (PCOM_ERR_ARG otherwise). */
 int pcom_gpu_cnn_features(pcom_handle *h, void *x_bf16, const pcom_cnn_stats *stats);
 /* Training target: (truth - pred) / dt / out_std per channel into FP32
  * [nk][glo_nj][glo_ni][4] (device), and the wet mask (U points for u, v, T
@@ -265,7 +266,8 @@ int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, fl
 /* Apply the network's output y (FP32 [nk][glo_nj][glo_ni][4], device) as a
  * tendency over dt seconds: uc, up += dt out_gain[0] out_std[0] y0 (wet U
  * points, y clipped to +-out_clip when out_clip > 0), vc, vp likewise, tc,
- * tp, sc, sp on wet T cells. */
+ * tp, sc, sp on wet T cells.  y must be 16-byte aligned (PCOM_ERR_ARG
+ * otherwise). */
 int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *stats, double dt);
 
 /* --- batches -------------------------------------------------------------- */

@@ -239,26 +239,33 @@ struct CnnStatsDev {
   double alpha_ref[64];
 };
 __device__ __forceinline__ float clip_y(float y, float c) { return c > 0.f ? fminf(fmaxf(y, -c), c) : y; }
-// R: the handle's 3-D storage (the mixed path stores alpha as alpha - alpha_r(k))
+__device__ __forceinline__ uint32_t bf16x2_bits(float lo, float hi) {
+  const __nv_bfloat162 b = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&b);
+}
+// The network's input at pixel (I, J, level k): grid (ceil(glo_ni / 128),
+// glo_nj, nk), one thread per pixel, its 16 BF16 channels written as two
+// 16-byte stores (16 separate 2-byte stores touched 32 sectors per warp
+// store).  R: the handle's 3-D storage (the mixed path stores alpha as
+// alpha - alpha_r(k)).
 template <typename R>
 __global__ void k_cnn_features(const __grid_constant__ DevT<R> P, __nv_bfloat16 *x, CnnStatsDev st) {
   constexpr bool MIXED = std::is_same<R, float>::value;
-  const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int I = (int)(p % P.glo_ni), J = (int)((p / P.glo_ni) % P.glo_nj), k = (int)(p / ((long long)P.glo_ni * P.glo_nj)) + 1;
-    const long long q2 = (long long)(I + 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
-    const bool wu = P.lev_u[q2] >= k, wt = P.lev_t[q2] >= k;
-    float v[5];
-    const double al = MIXED ? (double)P.alpha[q] + P.alpha_r[k] : (double)P.alpha[q];
-    v[0] = wu ? (float)(((double)P.uc[q] - st.in_mean[0]) / st.in_std[0]) : 0.f;
-    v[1] = wu ? (float)(((double)P.vc[q] - st.in_mean[1]) / st.in_std[1]) : 0.f;
-    v[2] = wt ? (float)(((double)P.tc[q] - st.in_mean[2]) / st.in_std[2]) : 0.f;
-    v[3] = wt ? (float)(((double)P.sc[q] - st.in_mean[3]) / st.in_std[3]) : 0.f;
-    v[4] = wt ? (float)((al - st.alpha_ref[k - 1] - st.in_mean[4]) / st.in_std[4]) : 0.f;
-    __nv_bfloat16 *o = x + p * 16;
-    #pragma unroll
-    for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16(c < 5 ? v[c] : 0.f);
-  }
+  const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y, k = blockIdx.z + 1;
+  if (I >= P.glo_ni) return;
+  const long long p = ((long long)(k - 1) * P.glo_nj + J) * P.glo_ni + I;
+  const long long q2 = (long long)(I + 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
+  const bool wu = P.lev_u[q2] >= k, wt = P.lev_t[q2] >= k;
+  float v[5];
+  const double al = MIXED ? (double)P.alpha[q] + P.alpha_r[k] : (double)P.alpha[q];
+  v[0] = wu ? (float)(((double)P.uc[q] - st.in_mean[0]) / st.in_std[0]) : 0.f;
+  v[1] = wu ? (float)(((double)P.vc[q] - st.in_mean[1]) / st.in_std[1]) : 0.f;
+  v[2] = wt ? (float)(((double)P.tc[q] - st.in_mean[2]) / st.in_std[2]) : 0.f;
+  v[3] = wt ? (float)(((double)P.sc[q] - st.in_mean[3]) / st.in_std[3]) : 0.f;
+  v[4] = wt ? (float)((al - st.alpha_ref[k - 1] - st.in_mean[4]) / st.in_std[4]) : 0.f;
+  uint4 *o = reinterpret_cast<uint4 *>(x + p * 16);
+  o[0] = make_uint4(bf16x2_bits(v[0], v[1]), bf16x2_bits(v[2], v[3]), bf16x2_bits(v[4], 0.f), 0u);
+  o[1] = make_uint4(0u, 0u, 0u, 0u);
 }
 __global__ void k_cnn_target(const __grid_constant__ Dev Pp, const __grid_constant__ Dev Pt, float *target, float *mask,
                              CnnStatsDev st, double rdt) {
@@ -281,31 +288,32 @@ __global__ void k_cnn_target(const __grid_constant__ Dev Pp, const __grid_consta
     }
   }
 }
+// the network's tendency applied at pixel (I, J, level k), the same grid
 template <typename R>
 __global__ void k_cnn_apply(const __grid_constant__ DevT<R> P, const float *y, CnnStatsDev st, double dt, int tp_distinct) {
-  const long long n = (long long)P.glo_ni * P.glo_nj * P.nk;
   const Grid2 G{P.ni, P.glo_ni, P.glo_nj, P.nk, P.n2};
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int I = (int)(p % P.glo_ni), J = (int)((p / P.glo_ni) % P.glo_nj), k = (int)(p / ((long long)P.glo_ni * P.glo_nj)) + 1;
-    const int i = I + 2;
-    const long long q2 = (long long)(i - 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
-    if (P.lev_u[q2] >= k) {
-      const double du = dt * st.out_gain[0] * st.out_std[0] * clip_y(y[p * 4 + 0], st.out_clip);
-      const double dv = dt * st.out_gain[1] * st.out_std[1] * clip_y(y[p * 4 + 1], st.out_clip);
-      put_twin(P.uc, G, i, q, (R)(P.uc[q] + du));
-      put_twin(P.vc, G, i, q, (R)(P.vc[q] + dv));
-      put_twin(P.up, G, i, q, (R)(P.up[q] + du));
-      put_twin(P.vp, G, i, q, (R)(P.vp[q] + dv));
-    }
-    if (P.lev_t[q2] >= k) {
-      const double dT = dt * st.out_gain[2] * st.out_std[2] * clip_y(y[p * 4 + 2], st.out_clip);
-      const double dS = dt * st.out_gain[3] * st.out_std[3] * clip_y(y[p * 4 + 3], st.out_clip);
-      put_twin(P.tc, G, i, q, (R)(P.tc[q] + dT));
-      put_twin(P.sc, G, i, q, (R)(P.sc[q] + dS));
-      if (tp_distinct) {
-        put_twin(P.tp, G, i, q, (R)(P.tp[q] + dT));
-        put_twin(P.sp, G, i, q, (R)(P.sp[q] + dS));
-      }
+  const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y, k = blockIdx.z + 1;
+  if (I >= P.glo_ni) return;
+  const long long p = ((long long)(k - 1) * P.glo_nj + J) * P.glo_ni + I;
+  const int i = I + 2;
+  const long long q2 = (long long)(i - 1) + (long long)P.ni * (J + 1), q = q2 + P.n2 * (k - 1);
+  const float4 yv = reinterpret_cast<const float4 *>(y)[p];
+  if (P.lev_u[q2] >= k) {
+    const double du = dt * st.out_gain[0] * st.out_std[0] * clip_y(yv.x, st.out_clip);
+    const double dv = dt * st.out_gain[1] * st.out_std[1] * clip_y(yv.y, st.out_clip);
+    put_twin(P.uc, G, i, q, (R)(P.uc[q] + du));
+    put_twin(P.vc, G, i, q, (R)(P.vc[q] + dv));
+    put_twin(P.up, G, i, q, (R)(P.up[q] + du));
+    put_twin(P.vp, G, i, q, (R)(P.vp[q] + dv));
+  }
+  if (P.lev_t[q2] >= k) {
+    const double dT = dt * st.out_gain[2] * st.out_std[2] * clip_y(yv.z, st.out_clip);
+    const double dS = dt * st.out_gain[3] * st.out_std[3] * clip_y(yv.w, st.out_clip);
+    put_twin(P.tc, G, i, q, (R)(P.tc[q] + dT));
+    put_twin(P.sc, G, i, q, (R)(P.sc[q] + dS));
+    if (tp_distinct) {
+      put_twin(P.tp, G, i, q, (R)(P.tp[q] + dT));
+      put_twin(P.sp, G, i, q, (R)(P.sp[q] + dS));
     }
   }
 }
@@ -1582,8 +1590,10 @@ int pcom_gpu_coarsen(pcom_handle *f, pcom_handle *c, int32_t factor) {
 
 int pcom_gpu_cnn_features(pcom_handle *h, void *x, const pcom_cnn_stats *st) {
   if (!h || !x || !st) return fail(PCOM_ERR_ARG, "null argument");
-  if (h->mixed) k_cnn_features<float><<<592, 256, 0, h->stream>>>(h->DM, (__nv_bfloat16 *)x, stats_dev(st));
-  else k_cnn_features<double><<<592, 256, 0, h->stream>>>(h->D, (__nv_bfloat16 *)x, stats_dev(st));
+  if ((uintptr_t)x & 15u) return fail(PCOM_ERR_ARG, "x must be 16-byte aligned");
+  const dim3 grid((unsigned)((h->dims.glo_ni + 127) / 128), (unsigned)h->dims.glo_nj, (unsigned)h->nk);
+  if (h->mixed) k_cnn_features<float><<<grid, 128, 0, h->stream>>>(h->DM, (__nv_bfloat16 *)x, stats_dev(st));
+  else k_cnn_features<double><<<grid, 128, 0, h->stream>>>(h->D, (__nv_bfloat16 *)x, stats_dev(st));
   CK(cudaGetLastError());
   h->launches++;
   return PCOM_OK;
@@ -1603,10 +1613,12 @@ int pcom_gpu_cnn_target(pcom_handle *pred, pcom_handle *truth, float *target, fl
 
 int pcom_gpu_cnn_apply(pcom_handle *h, const float *y, const pcom_cnn_stats *st, double dt) {
   if (!h || !y || !st) return fail(PCOM_ERR_ARG, "null argument");
+  if ((uintptr_t)y & 15u) return fail(PCOM_ERR_ARG, "y must be 16-byte aligned");
+  const dim3 grid((unsigned)((h->dims.glo_ni + 127) / 128), (unsigned)h->dims.glo_nj, (unsigned)h->nk);
   if (h->mixed)
-    k_cnn_apply<float><<<592, 256, 0, h->stream>>>(h->DM, y, stats_dev(st), dt, h->DM.tp != h->DM.tc ? 1 : 0);
+    k_cnn_apply<float><<<grid, 128, 0, h->stream>>>(h->DM, y, stats_dev(st), dt, h->DM.tp != h->DM.tc ? 1 : 0);
   else
-    k_cnn_apply<double><<<592, 256, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
+    k_cnn_apply<double><<<grid, 128, 0, h->stream>>>(h->D, y, stats_dev(st), dt, h->D.tp != h->D.tc ? 1 : 0);
   CK(cudaGetLastError());
   h->launches++;
   return PCOM_OK;

@@ -78,3 +78,64 @@ def test_closure_free_run_beats_plain():
     assert form["fell_back_at_step"] is None
     assert form["rms_mean"]["tc"] < plain
     net.close()
+
+
+def _f32(x):
+    return np.float64(np.float32(x))
+
+
+def test_features_and_apply_match_numpy():
+    """The network's input features and the tendency application, bit for
+    bit against a numpy restatement of their arithmetic on the FP64 path:
+    (x - mean) / std in FP64, rounded to FP32 then BF16 (round to nearest
+    even), zero on land and in channels 5..15; and x += dt gain std clip(y)
+    on the wet U (u, v) and T (T, S) points of the current and previous
+    levels."""
+    import torch
+
+    from pcom_b200.closure import _stats_struct
+
+    c = make_case("global1")
+    m = Model(c)
+    m.run(3)
+    H, W, nk = c["glo_nj"], c["glo_ni"], c["nk"]
+    rng = np.random.default_rng(4)
+    st = dict(in_mean=[0.003, -0.002, 12.5, 34.8, 1.3e-5], in_std=[0.07, 0.05, 6.3, 0.41, 7e-5],
+              out_std=[2e-6, 3e-6, 4e-5, 1e-6], out_gain=[0.5, 1.0, 0.75, 0.25], out_clip=2.5,
+              alpha_ref=list(rng.normal(0.0, 1e-5, nk)))
+    s = _stats_struct(st)
+    lib = L.load()
+    x = torch.full((nk * H * W, 16), 7.0, dtype=torch.bfloat16, device="cuda")
+    L.check(lib.pcom_gpu_cnn_features(m.handle, C.c_void_p(x.data_ptr()), C.byref(s)), "features")
+    torch.cuda.synchronize()
+    got = x.view(torch.int16).cpu().numpy().reshape(nk, H, W, 16)
+    sta = m.static()
+    k = np.arange(1, nk + 1)[:, None, None]
+    wu = sta["lev_u"][None, 1:-1, 1:-1] >= k
+    wt = sta["lev_t"][None, 1:-1, 1:-1] >= k
+    f = {n: m.field(n)[:, 1:-1, 1:-1] for n in ("uc", "vc", "tc", "sc", "alpha")}
+    mean, std = [_f32(v) for v in st["in_mean"]], [_f32(v) for v in st["in_std"]]
+    aref = np.asarray(st["alpha_ref"])[:, None, None]
+    ref = np.zeros((nk, H, W, 16), dtype=np.float32)
+    for ch, (name, w) in enumerate((("uc", wu), ("vc", wu), ("tc", wt), ("sc", wt))):
+        ref[..., ch] = np.where(w, ((f[name] - mean[ch]) / std[ch]), 0.0).astype(np.float32)
+    ref[..., 4] = np.where(wt, ((f["alpha"] - aref - mean[4]) / std[4]), 0.0).astype(np.float32)
+    want = torch.from_numpy(ref).to(torch.bfloat16).view(torch.int16).numpy()
+    assert np.array_equal(got, want), f"{np.count_nonzero(got != want)} features differ"
+
+    y = torch.from_numpy(rng.normal(0.0, 2.0, (nk * H * W, 4)).astype(np.float32)).cuda()
+    names = ("uc", "up", "vc", "vp", "tc", "tp", "sc", "sp")
+    before = {n: m.field(n)[:, 1:-1, 1:-1] for n in names}
+    dt = 3600.0
+    L.check(lib.pcom_gpu_cnn_apply(m.handle, C.c_void_p(y.data_ptr()), C.byref(s), C.c_double(dt)), "apply")
+    torch.cuda.synchronize()
+    yv = y.cpu().numpy().reshape(nk, H, W, 4)
+    clip = np.float32(st["out_clip"])
+    for ch, (a, b, w) in enumerate((("uc", "up", wu), ("vc", "vp", wu), ("tc", "tp", wt), ("sc", "sp", wt))):
+        yc = np.minimum(np.maximum(yv[..., ch], -clip), clip).astype(np.float64)
+        d = dt * _f32(st["out_gain"][ch]) * _f32(st["out_std"][ch]) * yc
+        for n in (a, b):
+            after = m.field(n)[:, 1:-1, 1:-1]
+            want = np.where(w, before[n] + d, before[n])
+            assert np.array_equal(after, want), f"{n}: {np.count_nonzero(after != want)} points differ"
+    m.close()
