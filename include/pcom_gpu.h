@@ -227,6 +227,16 @@ int pcom_gpu_global_sums(pcom_handle *h, double *out3);
 /* Use an external CUDA stream (cudaStream_t as void*) for all work. */
 int pcom_gpu_set_stream(pcom_handle *h, void *stream);
 int pcom_gpu_sync(pcom_handle *h);
+/* Latency floor of the barotropic subcycle: one launch of the resident FP64
+ * kernel's synchronisation skeleton.  It has the same grid, block and
+ * shared memory, and per substep the same ring reload, the seven CTA
+ * barriers, the interior stores and the grid barrier, without the
+ * arithmetic.  Its device time in milliseconds for the handle's nstep
+ * substeps goes to *ms (CUDA events; the call synchronises the handle's
+ * stream).  The model state is unchanged: the skeleton writes only the
+ * subcycle's scratch buffers.  PCOM_ERR_STATE unless the handle runs the
+ * resident FP64 kernel.  No counterpart in the reference. */
+int pcom_gpu_trop_floor(pcom_handle *h, double *ms);
 /* Per-kernel device timing with CUDA events (off by default).  When on,
  * pcom_gpu_profile_read fills up to `cap` entries of names (64 chars each),
  * launch counts and total milliseconds and returns the entry count. */

@@ -104,6 +104,7 @@ SIGNATURES = {
     "pcom_gpu_check_finite": (C.c_int, [C.c_void_p]),
     "pcom_gpu_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pcom_gpu_sync": (C.c_int, [C.c_void_p]),
+    "pcom_gpu_trop_floor": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "pcom_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcom_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64), dbl_p, C.c_int32]),
     "pcom_gpu_launch_count": (C.c_int64, [C.c_void_p]),

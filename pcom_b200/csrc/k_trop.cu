@@ -982,6 +982,74 @@ __global__ void __launch_bounds__(kResThreads, 1)
 }
 
 
+// The resident kernel's synchronisation skeleton, its latency floor: the
+// same grid, block and shared memory (so the same residency, one CTA per SM),
+// and per substep the same ring reload of ch, ub, vb from L2, the same seven
+// CTA barriers, the same interior stores and the same grid barrier on the
+// monotone arrival counter, with none of the arithmetic.  It writes only the
+// subcycle's ping-pong buffers, which every barotropic launch starts afresh
+// from chp, ubp, vbp.  (The real kernel also does the next substep's S2 on
+// its own points while it waits at the grid barrier.)
+__global__ void __launch_bounds__(kResThreads, 1)
+    k_trop_floor(const __grid_constant__ Dev P, int TX, int TY, int ntx, unsigned long long epoch) {
+  extern __shared__ double sm[];
+  __shared__ int s_stop;
+  const int nj = P.nj, G = P.glo_ni;
+  const int W = TX + 4, H = TY + 4, RS = W * H;
+  const int tid = threadIdx.x;
+  const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+  const int R0 = tx * TX, J0 = ty * TY + 1;
+  const int tw = min(TX, G - R0), th = min(TY, nj - J0 + 1);
+  const int rr0 = R0 - 2, jj0 = J0 - 2;
+  auto ring_i = [&](int r) { r %= G; if (r < 0) r += G; return r + 2; };
+  auto S = [&](int f, int p) -> double & { return sm[f * RS + p]; };
+  const int p = tid;
+  const int lx = p % W, ly = p / W;
+  const int j = jj0 + ly;
+  const bool active = p < RS && j >= 1 && j <= nj;
+  const int i = active ? ring_i(rr0 + lx) : 2;
+  const long long q = active ? I2(P, i, j) : 0;
+  const bool inS2 = active && lx < tw + 3 && ly < th + 3;
+  const bool inS8 = active && lx >= 2 && lx < tw + 2 && ly >= 2 && ly < th + 2;
+  __syncthreads();
+  for (int nt = 1; nt <= P.nstep; ++nt) {
+    const int d = (nt - 1) & 1;
+    const double *src_ch = (nt == 1) ? P.chp : P.tr_ch[1 - d];
+    const double *src_ub = (nt == 1) ? P.ubp : P.tr_ub[1 - d];
+    const double *src_vb = (nt == 1) ? P.vbp : P.tr_vb[1 - d];
+    if (active && (nt == 1 || !inS8)) {
+      S(R_CH, p) = __ldcg(src_ch + q);
+      if (inS2) { S(R_UB, p) = __ldcg(src_ub + q); S(R_VB, p) = __ldcg(src_vb + q); }
+    }
+    #pragma unroll 1
+    for (int b = 0; b < 5; ++b) __syncthreads();  // after S1, S2, S4, S5, S6
+    if (inS8) {
+      st2(P.tr_ch[d], P, i, q, S(R_CH, p));
+      st2(P.tr_ub[d], P, i, q, S(R_UB, p));
+      st2(P.tr_vb[d], P, i, q, S(R_VB, p));
+    }
+    __syncthreads();
+    if (tid == 0) {
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> c(*P.tile_flag);
+      c.fetch_add(1ULL, cuda::memory_order_release);
+      const unsigned long long want = epoch + (unsigned long long)nt * gridDim.x;
+      s_stop = wait_count(P.tile_flag, want, P.err, P.wait_ns) ? 0 : 1;
+    }
+    __syncthreads();
+    if (s_stop) return;
+  }
+}
+
+cudaError_t launch_trop_floor(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s) {
+  const int ntx = (P.glo_ni + TX - 1) / TX, nty = (P.nj + TY - 1) / TY;
+  const size_t smem = trop_fast_smem_bytes(TX, TY);
+  cudaError_t e = cudaFuncSetAttribute(k_trop_floor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int nthreads = ((TX + 4) * (TY + 4) + 31) / 32 * 32;
+  void *args[] = {(void *)&P, (void *)&TX, (void *)&TY, (void *)&ntx, (void *)&epoch};
+  return cudaLaunchCooperativeKernel((const void *)k_trop_floor, dim3(ntx * nty), dim3(nthreads), args, smem, s);
+}
+
 size_t trop_fast_smem_bytes(int TX, int TY) {
   return ((size_t)R_COUNT * (TX + 4) * (TY + 4) + 8 * (TX + 4) + 19 * (TY + 4)) * sizeof(double);
 }

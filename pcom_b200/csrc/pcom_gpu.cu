@@ -1691,6 +1691,33 @@ int pcom_gpu_sync(pcom_handle *h) {
   return sync_check(h);
 }
 
+int pcom_gpu_trop_floor(pcom_handle *h, double *ms) {
+  if (!h || !ms) return fail(PCOM_ERR_ARG, "null argument");
+  if (!h->static_ok) return fail(PCOM_ERR_STATE, "latency floor before pcom_gpu_upload_static");
+  if (h->trop_blocks <= 0) {
+    int rc = pick_trop_config(h);
+    if (rc) return rc;
+  }
+  if (!h->trop_resident || h->mixed)
+    return fail(PCOM_ERR_STATE, "the latency floor is measured for the resident FP64 barotropic kernel");
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, h->stream));
+  cudaError_t e = launch_trop_floor(h->D, h->trop_tx, h->trop_ty, h->trop_epoch, h->stream);
+  if (e == cudaSuccess) h->trop_epoch += (unsigned long long)h->D.nstep * (unsigned long long)h->trop_blocks;
+  CK(cudaEventRecord(e1, h->stream));
+  int rc = sync_check(h);
+  float t = 0.f;
+  if (rc == PCOM_OK && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return fail(PCOM_ERR_CUDA, "latency-floor kernel launch: %s", cudaGetErrorString(e));
+  if (rc) return rc;
+  *ms = t;
+  return PCOM_OK;
+}
+
 int pcom_gpu_profile(pcom_handle *h, int32_t enable) {
   if (!h) return fail(PCOM_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(h->stream));

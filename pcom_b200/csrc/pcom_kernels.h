@@ -45,6 +45,8 @@ int trop_res_max_blocks(int TX, int TY);
 // the same with reciprocal divisions (handle path)
 size_t trop_fast_smem_bytes(int TX, int TY);
 cudaError_t launch_trop_fast(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
+// the resident kernel's synchronisation skeleton (latency floor), same grid
+cudaError_t launch_trop_floor(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
 int trop_fast_max_blocks(int TX, int TY);
 // mixed path: the resident kernel with FP32 arithmetic outside the bottom pressure
 cudaError_t launch_trop_mixed(const Dev &P, int TX, int TY, unsigned long long epoch, cudaStream_t s);
