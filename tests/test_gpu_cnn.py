@@ -61,6 +61,47 @@ def test_conv_layer(cin, nout, mode, px):
         assert np.abs(got - ref).max() <= 2 ** -8 * scale + 1e-6
 
 
+def _conv_case(cin, nout, mode, px, h, w, nimg, seed):
+    """One convolution through the C ABI against the CPU restatement; the
+    largest error over the scale of the reference."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    npix = h * w * nimg
+    xd, x = bf16(rng.standard_normal((npix, cin)))
+    wd, wt = bf16(rng.standard_normal((9, nout, cin)) / np.sqrt(9 * cin))
+    b = rng.standard_normal(nout).astype(np.float32)
+    bd = torch.from_numpy(b).cuda()
+    auxd, aux = bf16(rng.standard_normal((npix, nout)))
+    nstore = 4 if mode == 1 else 0
+    if mode == 1:
+        outd = torch.zeros((npix, nstore), dtype=torch.float32, device="cuda")
+    else:
+        outd = torch.zeros((npix, nout), dtype=torch.bfloat16, device="cuda")
+    rc = L.load().pcom_cnn_conv_layer(cin, nout, xd.data_ptr(), wd.data_ptr(), bd.data_ptr(),
+                                      auxd.data_ptr() if mode == 2 else None, outd.data_ptr(), npix, h, w, px, mode,
+                                      nstore, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    cnn_check(rc, "conv")
+    ref = pycnn.conv(cin, nout, x, wt, b, aux if mode == 2 else None, h, w, px, mode, nstore)
+    got = outd.float().cpu().numpy()
+    return np.abs(got - ref).max() / np.abs(ref).max()
+
+
+# Image shapes at the edges of the row kernel's bookkeeping: one-row and
+# two-row images (every input row starts or ends an image), widths of
+# exactly one and two 128-pixel tiles (the wrapped right-halo pixel is the
+# slot's last row), one pixel over a tile, and a ragged second tile column.
+@pytest.mark.parametrize("h,w,nimg", [(1, 130, 4), (2, 128, 3), (5, 256, 2), (3, 200, 2), (7, 129, 2)])
+@pytest.mark.parametrize("px", [0, 1])
+@pytest.mark.parametrize("cin,nout,mode", [(64, 64, 0), (16, 64, 0), (64, 16, 1), (64, 64, 2)])
+def test_conv_layer_edge_shapes(cin, nout, mode, px, h, w, nimg):
+    rel = _conv_case(cin, nout, mode, px, h, w, nimg, seed=h * 1000 + w + 7 * cin + nout + mode)
+    if mode == 1:
+        assert rel <= 1e-5
+    else:
+        assert rel <= 2 ** -8 + 1e-6
+
+
 @pytest.mark.parametrize("cin,nout", [(16, 64), (64, 64), (64, 16)])
 def test_conv_partial_image(cin, nout):
     """A pixel count that is not whole images takes the per-tap tile form."""
