@@ -642,7 +642,10 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat
           if (ok && v1 && nw1 && q0 - 1 >= kBlocks)
             ok = mbar_spin(smem_u32(&bempty[7 - ((q0 - 1) & 7)]), (uint32_t)((((q0 - 1) >> 3) - 1) & 1));
           if (ok && !(pre && (pre_ok & 1u))) ok = mbar_spin(smem_u32(&full[s]), ph);
-          if (!ok || s_stop) {
+          // another role's stop is seen within 8 rows (a shared-memory read
+          // waits behind the MMAs' operand reads; this thread's own waits
+          // are bounded either way)
+          if (!ok || ((i & 7) == 0 && s_stop)) {
             if (!ok) stop();
             go = false;
             break;
@@ -660,7 +663,10 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_conv_rows(const __nv_bfloat
           // between targets 0 and 1 or 1 and 2
           const int r2 = (ta == 0 && tb >= 1 && (q0 & 7) == 0) ? 1 : ((ta <= 1 && tb == 2 && ((q0 - 1) & 7) == 0) ? 2 : -1);
           const uint32_t a_lo = a_lo0 + (uint32_t)s * SLOT16;
-          fence_async_smem();
+          // cp.async rows (generic proxy) need a proxy fence before the
+          // MMAs read them; tensor-loaded rows are async-proxy writes and
+          // their halo writer fences before it releases the slot
+          if (!row_tma<CIN>()) fence_async_smem();
           tc_fence_after();
           if (ta == 0 && tb == 2 && r2 < 0 && !nw1) {
             // the common row: outputs i + 1, i, i - 1 in adjacent blocks, only
