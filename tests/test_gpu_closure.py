@@ -84,19 +84,22 @@ def _f32(x):
     return np.float64(np.float32(x))
 
 
-def test_features_and_apply_match_numpy():
+@pytest.mark.parametrize("flags", [L.PCOM_PREC_FP64, L.PCOM_PREC_MIXED], ids=["fp64", "mixed"])
+def test_features_and_apply_match_numpy(flags):
     """The network's input features and the tendency application, bit for
-    bit against a numpy restatement of their arithmetic on the FP64 path:
-    (x - mean) / std in FP64, rounded to FP32 then BF16 (round to nearest
-    even), zero on land and in channels 5..15; and x += dt gain std clip(y)
-    on the wet U (u, v) and T (T, S) points of the current and previous
-    levels."""
+    bit against a numpy restatement of their arithmetic: (x - mean) / std in
+    FP64 (alpha as stored plus the reference profile on the mixed path),
+    rounded to FP32 then BF16 (round to nearest even), zero on land and in
+    channels 5..15; and x += dt gain std clip(y) in FP64 on the wet U (u, v)
+    and T (T, S) points of the current and previous levels, rounded to the
+    handle's storage."""
     import torch
 
     from pcom_b200.closure import _stats_struct
 
     c = make_case("global1")
-    m = Model(c)
+    m = Model(c, flags=flags)
+    store = np.float32 if flags == L.PCOM_PREC_MIXED else np.float64
     m.run(3)
     H, W, nk = c["glo_nj"], c["glo_ni"], c["nk"]
     rng = np.random.default_rng(4)
@@ -136,6 +139,6 @@ def test_features_and_apply_match_numpy():
         d = dt * _f32(st["out_gain"][ch]) * _f32(st["out_std"][ch]) * yc
         for n in (a, b):
             after = m.field(n)[:, 1:-1, 1:-1]
-            want = np.where(w, before[n] + d, before[n])
+            want = np.where(w, (before[n] + d).astype(store).astype(np.float64), before[n])
             assert np.array_equal(after, want), f"{n}: {np.count_nonzero(after != want)} points differ"
     m.close()
