@@ -144,7 +144,7 @@ def test_wgrad(cin, nout, px):
 
 
 # the 1-degree closure's images: one 160 x 360 level image per model level,
-# periodic in x (the production strip walk of the persistent kernel)
+# periodic in x (the production row walk of the persistent kernel)
 HF, WF, NF = 160, 360, 2
 
 
@@ -178,7 +178,7 @@ def test_conv_layer_full_shape(cin, nout, mode):
         assert np.abs(got - ref).max() <= 1e-5 * scale
     else:
         assert np.abs(got - ref).max() <= 2 ** -8 * scale + 1e-6
-    # every pixel was written (the strip walk covers the whole image)
+    # every pixel was written (the row walk covers the whole image)
     assert np.count_nonzero(np.abs(got - ref) > 2 ** -8 * scale + 1e-6) == 0
 
 
