@@ -16,7 +16,7 @@ Windows.  The fine run goes on through four consecutive windows: spin-up;
 training (samples every `every` coarse steps); validation (coarse runs with
 each output variant of VARIANTS, which picks the one applied); test (coarse
 runs of the chosen variant at each cadence, in the closure form's precision,
-beside the plain coarse model in FP64 and in that precision), judged by
+beside the plain coarse model in FP64 and in that precision), evaluated by
 the RMS error against CG(fine) averaged over the window.  The SYPD of each
 form comes from CUDA-event timings of its step and of the network.
 
@@ -411,7 +411,7 @@ def main():
     p.add_argument("--target-steps", type=int, default=1,
                    help="coarse steps the training residual is accumulated over")
     p.add_argument("--val-days", type=float, default=2, help="window that picks the applied outputs and gain")
-    p.add_argument("--test-days", type=float, default=2, help="window the chosen closure is judged on")
+    p.add_argument("--test-days", type=float, default=2, help="window the chosen closure is evaluated on")
     p.add_argument("--form-flags", default="fp64", choices=sorted(FLAGS),
                    help="precision of the closure form's coarse model")
     p.add_argument("--cadences", default="1", help="comma-separated: apply the network every k coarse steps")
