@@ -694,17 +694,22 @@ def ensemble_measure(args, steps: int, print_line: bool):
         d2h += 3 * n2 * 8
     first = it0 + 1 + 2 * steps
 
+    # the asynchronous calls, as in the single-domain e2e: each member's
+    # forcing staged on its upload stream, its state copied out on its
+    # download stream while the next batched step runs; one sync at the end
     def e2e_body():
         for q in range(steps):
             it = first + q
             for m, fo in zip(models, fos):
-                L.check(lib.pcom_gpu_set_forcing(m.handle, C.byref(fo)), "set_forcing")
+                L.check(lib.pcom_gpu_set_forcing_async(m.handle, C.byref(fo)), "set_forcing_async")
             if day_of(it) != day_of(it - 1):
                 b.den_prho()
             b.step_async(it)
-            b.sync()
             for m, st in zip(models, sts):
-                L.check(lib.pcom_gpu_get_state(m.handle, C.byref(st)), "get_state")
+                L.check(lib.pcom_gpu_get_state_async(m.handle, C.byref(st)), "get_state_async")
+        b.sync()
+        for m in models:
+            L.check(lib.pcom_gpu_sync(m.handle), "sync")  # the last states are in host memory
 
     t_e2e = timed(e2e_body)
     for m in models:

@@ -89,3 +89,57 @@ def test_async_forcing_requires_all_fields():
     with pytest.raises(L.PcomError):
         L.check(m.lib.pcom_gpu_set_forcing_async(m.handle, C.byref(fo)), "set_forcing_async")
     m.close()
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_batch_async_transfers_equal_sync(graphs):
+    """The same with a batch: every member's forcing staged with
+    set_forcing_async and its state copied out with get_state_async around
+    each batched step (CUDA graphs on and off) equals the batch driven
+    through the synchronous calls, per step and at the end."""
+    from pcom_b200.model import Batch
+    from pcom_b200.synth import perturb
+
+    base = make_case("tiny_bathy")
+    cases = [base, perturb(base, 1), make_case("tiny")]
+    nsteps = 7
+    runs = {}
+    for mode in ("sync", "async"):
+        ms = [Model(c) for c in cases]
+        lib = ms[0].lib
+        bt = Batch(ms, graphs=graphs)
+        fs = [_forcings(m, nsteps) for m in ms]
+        fo = [[_fo(f) for f in fm] for fm in fs]
+        outs = [[{k: np.full(m.field(k).size, np.nan) for k in OUT} for _ in range(nsteps)] for m in ms]
+        reqs = [[_state_req(m, o) for o in om] for m, om in zip(ms, outs)]
+        bt.den_prho()
+        for q in range(nsteps):
+            for mi, m in enumerate(ms):
+                if mode == "sync":
+                    L.check(lib.pcom_gpu_set_forcing(m.handle, C.byref(fo[mi][q])), "set_forcing")
+                else:
+                    L.check(lib.pcom_gpu_set_forcing_async(m.handle, C.byref(fo[mi][q])), "set_forcing_async")
+            bt.step_async(q + 1)
+            if mode == "sync":
+                bt.sync()
+            for mi, m in enumerate(ms):
+                if mode == "sync":
+                    L.check(lib.pcom_gpu_get_state(m.handle, C.byref(reqs[mi][q])), "get_state")
+                else:
+                    L.check(lib.pcom_gpu_get_state_async(m.handle, C.byref(reqs[mi][q])), "get_state_async")
+        bt.sync()
+        for m in ms:
+            L.check(lib.pcom_gpu_sync(m.handle), "sync")
+        runs[mode] = (ms, outs, bt)
+    (ma, oa, ba), (mb, ob, bb) = runs["sync"], runs["async"]
+    for mi in range(len(cases)):
+        for q in range(nsteps):
+            for k in OUT:
+                assert np.array_equal(oa[mi][q][k], ob[mi][q][k]), f"member {mi} step {q + 1}: {k} differs"
+        for f in STATE_FIELDS:
+            assert np.array_equal(ma[mi].field(f), mb[mi].field(f)), f"member {mi}: {f} differs"
+    assert not np.array_equal(oa[0][0]["ubc"], oa[0][-1]["ubc"])
+    for bt in (ba, bb):
+        bt.close()
+    for m in ma + mb:
+        m.close()
